@@ -1,0 +1,210 @@
+// C-ABI host runtime: contexts, device workspaces, host<->device staging and
+// kernel launches for the entry points declared in include/lcbinint_b200.h.
+#include "../../include/lcbinint_b200.h"
+#include "lcbi_context.h"
+#include "lcbi_kernels.h"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+using lcbi::Context;
+
+namespace lcbi {
+
+bool Context::fail(const char* what, cudaError_t e)
+{
+    error = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+bool Context::fail(const std::string& what)
+{
+    error = what;
+    return false;
+}
+
+bool Context::ensure(Buffer& b, size_t bytes)
+{
+    if (b.bytes >= bytes) return true;
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = bytes < 4096 ? 4096 : bytes;
+    want = (want + 0xffff) & ~size_t(0xffff);
+    const cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) return fail("cudaMalloc", e);
+    b.bytes = want;
+    return true;
+}
+
+bool Context::check(const char* what, cudaError_t e)
+{
+    if (e == cudaSuccess) return true;
+    return fail(what, e);
+}
+
+Context::~Context()
+{
+    cudaSetDevice(device);
+    for (Buffer* b : all_buffers()) {
+        if (b->ptr) cudaFree(b->ptr);
+    }
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// Stages `count` elements of an input array: device pointers pass through,
+// host arrays are copied into `buf`.
+template <typename T>
+bool Context::stage_in(Buffer& buf, const T* src, size_t count, bool device_ptrs, const T** out)
+{
+    if (device_ptrs) {
+        *out = src;
+        return true;
+    }
+    if (!ensure(buf, count * sizeof(T))) return false;
+    if (count && !check("cudaMemcpyAsync H2D",
+                        cudaMemcpyAsync(buf.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice, stream)))
+        return false;
+    *out = static_cast<const T*>(buf.ptr);
+    return true;
+}
+
+template <typename T>
+bool Context::stage_out(Buffer& buf, T* dst, size_t count, bool device_ptrs, T** out)
+{
+    if (device_ptrs || dst == nullptr) {
+        *out = dst;
+        return true;
+    }
+    if (!ensure(buf, count * sizeof(T))) return false;
+    *out = static_cast<T*>(buf.ptr);
+    return true;
+}
+
+template <typename T>
+bool Context::copy_back(T* dst, const T* dev, size_t count, bool device_ptrs)
+{
+    if (device_ptrs || dst == nullptr || count == 0) return true;
+    return check("cudaMemcpyAsync D2H", cudaMemcpyAsync(dst, dev, count * sizeof(T), cudaMemcpyDeviceToHost, stream));
+}
+
+bool Context::finish()
+{
+    return check("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+}
+
+template bool Context::stage_in<double>(Buffer&, const double*, size_t, bool, const double**);
+template bool Context::stage_in<int>(Buffer&, const int*, size_t, bool, const int**);
+template bool Context::stage_out<double>(Buffer&, double*, size_t, bool, double**);
+template bool Context::stage_out<int>(Buffer&, int*, size_t, bool, int**);
+template bool Context::copy_back<double>(double*, const double*, size_t, bool);
+template bool Context::copy_back<int>(int*, const int*, size_t, bool);
+
+} // namespace lcbi
+
+extern "C" {
+
+int lcbi_gpu_create(int device, lcbi_gpu_context** out)
+{
+    if (out == nullptr) return LCBI_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return LCBI_GPU_ERROR;
+    }
+    Context* ctx = new (std::nothrow) Context();
+    if (!ctx) return LCBI_GPU_ERROR;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return LCBI_GPU_ERROR;
+    }
+    *out = reinterpret_cast<lcbi_gpu_context*>(ctx);
+    return LCBI_OK;
+}
+
+void lcbi_gpu_destroy(lcbi_gpu_context* c)
+{
+    delete reinterpret_cast<Context*>(c);
+}
+
+const char* lcbi_gpu_last_error(const lcbi_gpu_context* c)
+{
+    return c ? reinterpret_cast<const Context*>(c)->error.c_str() : "null context";
+}
+
+int64_t lcbi_gpu_launch_count(const lcbi_gpu_context* c)
+{
+    return c ? reinterpret_cast<const Context*>(c)->launches : 0;
+}
+
+int lcbi_gpu_binary_mag0(lcbi_gpu_context* c, int64_t n, const double* s, const double* q, const double* y1,
+                         const double* y2, double* A, int32_t* image_count, int32_t* status, unsigned flags)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!s || !q || !y1 || !y2 || !A) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
+    const size_t N = static_cast<size_t>(n);
+    const double *ds, *dq, *dy1, *dy2;
+    double* dA;
+    int *dn, *dst;
+    if (!ctx->stage_in(ctx->in[0], s, N, dev, &ds) || !ctx->stage_in(ctx->in[1], q, N, dev, &dq) ||
+        !ctx->stage_in(ctx->in[2], y1, N, dev, &dy1) || !ctx->stage_in(ctx->in[3], y2, N, dev, &dy2) ||
+        !ctx->stage_out(ctx->out[0], A, N, dev, &dA) ||
+        !ctx->stage_out(ctx->out[1], reinterpret_cast<int*>(image_count), N, dev, &dn) ||
+        !ctx->stage_out(ctx->out[2], reinterpret_cast<int*>(status), N, dev, &dst))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("ps_batch_kernel", lcbi::launch_ps_batch(ds, dq, dy1, dy2, dA, dn, dst, n, ctx->sm_count,
+                                                             ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    if (!ctx->copy_back(A, dA, N, dev) || !ctx->copy_back(reinterpret_cast<int*>(image_count), dn, N, dev) ||
+        !ctx->copy_back(reinterpret_cast<int*>(status), dst, N, dev) || !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_binary_mag0_derivatives(lcbi_gpu_context* c, int64_t n, const double* s, const double* q,
+                                     const double* y1, const double* y2, double* A, int32_t* image_count,
+                                     double* indicator, unsigned flags)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!s || !q || !y1 || !y2 || !A || !image_count || !indicator) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
+    const size_t N = static_cast<size_t>(n);
+    const double *ds, *dq, *dy1, *dy2;
+    double *dA, *dind;
+    int* dn;
+    if (!ctx->stage_in(ctx->in[0], s, N, dev, &ds) || !ctx->stage_in(ctx->in[1], q, N, dev, &dq) ||
+        !ctx->stage_in(ctx->in[2], y1, N, dev, &dy1) || !ctx->stage_in(ctx->in[3], y2, N, dev, &dy2) ||
+        !ctx->stage_out(ctx->out[0], A, N, dev, &dA) ||
+        !ctx->stage_out(ctx->out[1], reinterpret_cast<int*>(image_count), N, dev, &dn) ||
+        !ctx->stage_out(ctx->out[2], indicator, N, dev, &dind))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("ps_deriv_kernel",
+                    lcbi::launch_ps_deriv(ds, dq, dy1, dy2, dA, dn, dind, n, ctx->sm_count, ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    if (!ctx->copy_back(A, dA, N, dev) || !ctx->copy_back(reinterpret_cast<int*>(image_count), dn, N, dev) ||
+        !ctx->copy_back(indicator, dind, N, dev) || !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+} // extern "C"

@@ -114,40 +114,32 @@ class _Lib:
         return r[0::2] + 1j * r[1::2]
 
 
-class Oracle(_Lib):
-    """The CPU restatement."""
+class _FsLib(_Lib):
+    """Finite-source entry points shared by the oracle and the reference shim."""
 
-    def __init__(self):
-        super().__init__(ORACLE_SO, "orc_")
-
-
-class Reference(_Lib):
-    """The reference compiled from its own sources (oracle/_ref)."""
-
-    def __init__(self):
-        super().__init__(REF_SO, "ref_")
-        L = self.lib
-        L.ref_binary_mag.argtypes = [C.POINTER(FsSettings)] + [C.c_double] * 6 + [C.c_int, _dp, _ip]
-        L.ref_inverse_ray_many.argtypes = [C.POINTER(FsSettings), C.c_int] + [_dp] * 6 + [_ip]
-        L.ref_seeds.argtypes = [C.POINTER(FsSettings)] + [C.c_double] * 5 + [_dp, C.c_int]
-        L.ref_seeds_phase12.argtypes = [C.c_double] * 5 + [_dp, C.c_int]
-        L.ref_cartesian.argtypes = [C.POINTER(FsSettings)] + [C.c_double] * 5 + [_dp, C.c_int, _dp]
-        L.ref_cartesian.restype = C.c_double
-        L.ref_polar.argtypes = [C.POINTER(FsSettings)] + [C.c_double] * 5 + [_dp, C.c_int]
-        L.ref_polar.restype = C.c_double
-        L.ref_hexadecapole.argtypes = [C.POINTER(FsSettings)] + [C.c_double] * 5 + [_dp, _dp]
-        L.ref_caustic_cache.argtypes = [C.c_double, C.c_double, C.c_int, _dp, C.c_int, _dp, _dp]
-        L.ref_caustic_distances.argtypes = [C.c_double] * 2 + [C.c_int] + [C.c_double] * 3 + [_dp]
-        L.ref_critical_sources.argtypes = [C.c_double] * 3 + [_dp]
-        L.ref_ld_brightness.argtypes = [C.c_double] * 3
-        L.ref_ld_brightness.restype = C.c_double
-        L.ref_light_curve_static.argtypes = ([C.POINTER(FsSettings), _dp, C.c_int] + [C.c_double] * 7
-                                             + [_dp, _ip])
+    def __init__(self, path, prefix):
+        super().__init__(path, prefix)
+        f = self.fn
+        st = C.POINTER(FsSettings)
+        f("binary_mag").argtypes = [st] + [C.c_double] * 6 + [C.c_int, _dp, _ip]
+        f("inverse_ray_many").argtypes = [st, C.c_int] + [_dp] * 6 + [_ip]
+        f("seeds").argtypes = [st] + [C.c_double] * 5 + [_dp, C.c_int]
+        f("cartesian").argtypes = [st] + [C.c_double] * 5 + [_dp, C.c_int, _dp]
+        f("cartesian").restype = C.c_double
+        f("polar").argtypes = [st] + [C.c_double] * 5 + [_dp, C.c_int]
+        f("polar").restype = C.c_double
+        f("hexadecapole").argtypes = [st] + [C.c_double] * 5 + [_dp, _dp]
+        f("caustic_cache").argtypes = [C.c_double, C.c_double, C.c_int, _dp, C.c_int, _dp, _dp]
+        f("caustic_distances").argtypes = [C.c_double] * 2 + [C.c_int] + [C.c_double] * 3 + [_dp]
+        f("critical_sources").argtypes = [C.c_double] * 3 + [_dp]
+        f("ld_brightness").argtypes = [C.c_double] * 3
+        f("ld_brightness").restype = C.c_double
+        f("light_curve_static").argtypes = [st, _dp, C.c_int] + [C.c_double] * 7 + [_dp, _ip]
 
     def binary_mag(self, st, s, q, x, y, rho, a_ps, ps_exact=True):
         d = np.zeros(2)
         i = np.zeros(4, dtype=np.int32)
-        self.lib.ref_binary_mag(C.byref(st), s, q, x, y, rho, a_ps, int(ps_exact), _ptr(d), _ptr(i, _ip))
+        self.fn("binary_mag")(C.byref(st), s, q, x, y, rho, a_ps, int(ps_exact), _ptr(d), _ptr(i, _ip))
         return dict(A=d[0], err=d[1], method=int(i[0]), level=int(i[1]), converged=bool(i[2]))
 
     def inverse_ray(self, st, s, q, x, y, rho):
@@ -156,29 +148,29 @@ class Reference(_Lib):
         n = s.size
         A = np.empty(n)
         m = np.empty(n, dtype=np.int32)
-        self.lib.ref_inverse_ray_many(C.byref(st), n, _ptr(s), _ptr(q), _ptr(x), _ptr(y), _ptr(rho),
-                                      _ptr(A), _ptr(m, _ip))
+        self.fn("inverse_ray_many")(C.byref(st), n, _ptr(s), _ptr(q), _ptr(x), _ptr(y), _ptr(rho),
+                                    _ptr(A), _ptr(m, _ip))
         return A, m
 
     def seeds(self, st, s, q, x, y, rho, cap=512):
         out = np.zeros(2 * cap)
-        n = self.lib.ref_seeds(C.byref(st), s, q, x, y, rho, _ptr(out), cap)
+        n = self.fn("seeds")(C.byref(st), s, q, x, y, rho, _ptr(out), cap)
         return out[: 2 * min(n, cap)].reshape(-1, 2)
 
     def cartesian(self, st, s, q, x, y, rho, seeds):
         sd = _f64(seeds).ravel()
         diag = np.zeros(8)
-        A = self.lib.ref_cartesian(C.byref(st), s, q, x, y, rho, _ptr(sd), sd.size // 2, _ptr(diag))
+        A = self.fn("cartesian")(C.byref(st), s, q, x, y, rho, _ptr(sd), sd.size // 2, _ptr(diag))
         return A, diag
 
     def polar(self, st, s, q, x, y, rho, seeds):
         sd = _f64(seeds).ravel()
-        return self.lib.ref_polar(C.byref(st), s, q, x, y, rho, _ptr(sd), sd.size // 2)
+        return self.fn("polar")(C.byref(st), s, q, x, y, rho, _ptr(sd), sd.size // 2)
 
     def hexadecapole(self, st, s, q, x, y, rho, a0=None):
         out = np.zeros(2)
         k = None if a0 is None else C.byref(C.c_double(a0))
-        self.lib.ref_hexadecapole(C.byref(st), s, q, x, y, rho, k, _ptr(out))
+        self.fn("hexadecapole")(C.byref(st), s, q, x, y, rho, k, _ptr(out))
         return out[0], out[1]
 
     def caustic_cache(self, s, q, bins=1400):
@@ -186,29 +178,43 @@ class Reference(_Lib):
         br = np.zeros(4 * cap * 2)
         bbox = np.zeros(4)
         ms = C.c_double()
-        per = self.lib.ref_caustic_cache(s, q, bins, _ptr(br), cap, _ptr(bbox), C.byref(ms))
+        per = self.fn("caustic_cache")(s, q, bins, _ptr(br), cap, _ptr(bbox), C.byref(ms))
         return br.reshape(4, cap, 2)[:, :per], bbox, ms.value
 
     def caustic_distances(self, s, q, x, y, search_radius, bins=1400):
         out = np.zeros(2)
-        self.lib.ref_caustic_distances(s, q, bins, x, y, search_radius, _ptr(out))
+        self.fn("caustic_distances")(s, q, bins, x, y, search_radius, _ptr(out))
         return out[0], out[1]
 
     def critical_sources(self, s, q, phi):
         out = np.zeros(8)
-        n = self.lib.ref_critical_sources(s, q, phi, _ptr(out))
+        n = self.fn("critical_sources")(s, q, phi, _ptr(out))
         return out[: 2 * n].reshape(-1, 2)
 
     def ld_brightness(self, c, d, r2):
-        return self.lib.ref_ld_brightness(c, d, r2)
+        return self.fn("ld_brightness")(c, d, r2)
 
     def light_curve_static(self, st, times, t0, tE, u0, alpha, s, q, rho):
         t = _f64(times)
         out = np.empty(t.size)
         m = np.empty(t.size, dtype=np.int32)
-        rc = self.lib.ref_light_curve_static(C.byref(st), _ptr(t), t.size, t0, tE, u0, alpha, s, q,
-                                             rho, _ptr(out), _ptr(m, _ip))
+        rc = self.fn("light_curve_static")(C.byref(st), _ptr(t), t.size, t0, tE, u0, alpha, s, q, rho,
+                                           _ptr(out), _ptr(m, _ip))
         return out, m, rc
+
+
+class Oracle(_FsLib):
+    """The CPU restatement."""
+
+    def __init__(self):
+        super().__init__(ORACLE_SO, "orc_")
+
+
+class Reference(_FsLib):
+    """The reference compiled from its own sources (oracle/_ref)."""
+
+    def __init__(self):
+        super().__init__(REF_SO, "ref_")
 
 
 def import_reference_module():

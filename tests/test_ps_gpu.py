@@ -53,7 +53,7 @@ def test_bit_exact_vs_oracle(oracle_lib, seed, invert):
 def test_derivative_indicator_bit_exact(oracle_lib):
     import lcbinint_b200 as lb
     from lcbinint_b200 import _lib
-    s, q, y1, y2 = _cfg2_points(50_000, 2)
+    s, q, y1, y2 = (np.ascontiguousarray(v) for v in _cfg2_points(50_000, 2))
     ctx = lb.context()
     n = s.size
     A = np.empty(n); nimg = np.empty(n, dtype=np.int32); ind = np.empty(n)

@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""Benchmark of the lcbinint B200 magnification path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload fs_batch|ps_batch|light_curve]
+
+Default workload (fs_batch): the uneven finite-source batch -- 4,096 light-curve
+points from 64 random binary-lens models (s log-U[0.3,3], q log-U[1e-5,1], rho
+log-U[1e-4,1e-2], u0 U[-0.2,0.2], alpha U[0,2pi], linear limb darkening
+U[0,0.8]), 64 epochs per model spread over the caustic-crossing window,
+Cartesian or polar grid per point (p = 0.5) and nbin log-U{20..200}, every
+point integrated by inverse ray (lcbinint.binary_inverse_ray semantics), all
+points in one launch sequence, FP64.  One step = the whole batch.
+
+One JSON line on rank 0: value = magnifications/s with inputs resident on the
+GPU; e2e = the same through the host-pointer C ABI (host->device copies and
+result readback inside the timed region); roofline of the dominant kernel
+against the device-measured FP64 FMA peak; cpu_baseline = the reference
+compiled from source (oracle/_ref), one process per host core, on a bounded
+sample of the same points.  Under torchrun every rank runs its own batch
+(independent points: weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "finite-source mags/s & rays/s on 1 B200 at 1e-4 rel err; fwd+grad/fwd ratio"
+F_RAY = 32.0      # algorithmic flop per lens-map evaluation of one cell
+F_PS = 3500.0     # algorithmic FP64 flop per point-source solve
+
+# --------------------------------------------------------------------------- workloads
+
+
+def _critical_caustic_points(s, q_core, n_phase=256):
+    """Caustic points (centre-of-mass frame) from the critical-curve quartic, numpy only."""
+    qi = abs(q_core)
+    q = qi if qi < 1.0 else 1.0 / qi
+    a = -s if qi < 1.0 else s
+    m1 = 1.0 / (1.0 + q)
+    m2 = q * m1
+    pts = []
+    for phi in np.linspace(0.0, 2 * np.pi, n_phase, endpoint=False):
+        e = np.exp(1j * phi)
+        coef = [-e, 2 * e * a, m1 + m2 - e * a * a, -2 * m2 * a, m2 * a * a]
+        for z in np.roots(coef):
+            zc = np.conj(z)
+            y = z - m1 / (zc - a) - m2 / zc - a * m1
+            pts.append((y.real, y.imag))
+    return np.array(pts)
+
+
+def fs_batch_workload(seed=1, n_models=64, per_model=64):
+    rng = np.random.default_rng(seed)
+    rows = []
+    for _ in range(n_models):
+        s = float(np.exp(rng.uniform(np.log(0.3), np.log(3.0))))
+        q = float(np.exp(rng.uniform(np.log(1e-5), 0.0)))
+        rho = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2))))
+        u0 = float(rng.uniform(-0.2, 0.2))
+        alpha = float(rng.uniform(0.0, 2 * np.pi))
+        gam = float(rng.uniform(0.0, 0.8))
+        pts = _critical_caustic_points(s, 1.0 / q)
+        ca, sa = math.cos(alpha), math.sin(alpha)
+        # entry/exit of the trajectory through the caustic bounding box (+- 3 rho)
+        lo, hi = pts.min(axis=0) - 3 * rho, pts.max(axis=0) + 3 * rho
+        tau_lo, tau_hi = -np.inf, np.inf
+        for d, p0, a0, b0 in ((ca, -u0 * sa, lo[0], hi[0]), (sa, u0 * ca, lo[1], hi[1])):
+            if abs(d) < 1e-12:
+                if not (a0 <= p0 <= b0):
+                    tau_lo, tau_hi = np.inf, -np.inf
+                continue
+            t1, t2 = sorted(((a0 - p0) / d, (b0 - p0) / d))
+            tau_lo, tau_hi = max(tau_lo, t1), min(tau_hi, t2)
+        if not tau_lo < tau_hi:  # misses the box: span the box's projection on the trajectory
+            proj = pts @ np.array([ca, sa])
+            tau_lo, tau_hi = proj.min() - 3 * rho, proj.max() + 3 * rho
+        for tau in np.linspace(tau_lo, tau_hi, per_model):
+            x = tau * ca - u0 * sa
+            y = tau * sa + u0 * ca
+            polar = rng.random() < 0.5
+            nbin = int(round(math.exp(rng.uniform(math.log(20), math.log(200)))))
+            rows.append((s, 1.0 / q, x, y, rho, gam, 2 if polar else 1, nbin))
+    return np.array(rows)
+
+
+def fs_settings_for(rows):
+    from lcbinint_b200.api import LimbDarkening, Options
+    keys = {}
+    settings = []
+    idx = np.empty(len(rows), dtype=np.int32)
+    for i, r in enumerate(rows):
+        k = (float(r[5]), int(r[6]), int(r[7]))
+        if k not in keys:
+            keys[k] = len(settings)
+            o = Options(inverse_ray_grid="polar" if k[1] == 2 else "cartesian", nbin=k[2])
+            st = o.fs_settings(LimbDarkening.linear(k[0]))
+            # lcbinint.binary_inverse_ray thresholds (python/lcbinint_pybind.cpp:3831-3833)
+            st.kinji_threshold = 1e18
+            st.hex_threshold = 0.0
+            st.adaptive_hex_threshold = 0.0
+            settings.append(st)
+        idx[i] = keys[k]
+    return settings, idx
+
+
+# --------------------------------------------------------------------------- helpers
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2(buf):
+    buf.add_(1.0)  # writes 256 MB (> 126 MB L2) between timed steps
+
+
+# --------------------------------------------------------------------------- CPU reference
+
+
+def _ref_worker(args):
+    """One process (the reference solver keeps static state): forced inverse ray on a chunk."""
+    rows, = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Reference, default_settings
+    ref = Reference()
+    t = time.perf_counter()
+    out = []
+    for r in rows:
+        st = default_settings(source_bins=int(r[7]), finite_mode=int(r[6]), limb_darkening_c=float(r[5]))
+        A, _ = ref.inverse_ray(st, r[0], r[1], r[2], r[3], r[4])
+        out.append(A[0])
+    return time.perf_counter() - t, out
+
+
+def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
+    """Points/s of the reference on a bounded random sample, one process per core.
+
+    The sample is grown until the pool's wall time reaches about target_seconds."""
+    import multiprocessing as mp
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(rows))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n_procs) as pool:
+        # calibrate on one point per process
+        take = order[:n_procs]
+        t0 = time.perf_counter()
+        pool.map(_ref_worker, [([rows[i]],) for i in take])
+        cal = time.perf_counter() - t0
+        per_point = max(cal, 1e-3)  # one point per process in parallel
+        m = int(max(1, min(len(rows) // n_procs, target_seconds / per_point)))
+        sample = order[: m * n_procs]
+        chunks = [([rows[i] for i in sample[k::n_procs]],) for k in range(n_procs)]
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, chunks)
+        wall = time.perf_counter() - t0
+    n = sum(len(c[0]) for c in chunks)
+    return n / wall, n, wall
+
+
+# --------------------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=0,
+                    help="use only the first N points (small cases for profiler captures)")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+    rows = fs_batch_workload(seed=1 + rank)
+    if args.points > 0:
+        rows = rows[np.random.default_rng(5).permutation(len(rows))[: args.points]]
+    config = {"workload": "fs_batch: 4096 forced inverse-ray points, 64 models x 64 epochs, "
+                          "Cartesian/polar mixed, nbin 20-200, linear LD",
+              "points": int(len(rows)), "models": 64, "precision": "fp64 (bit-exact vs reference)",
+              "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per_step = []
+        for _ in range(args.warmup + args.steps):
+            rate, n, wall = cpu_reference_rate(rows, ncores, target_seconds=max(2.0, args.cpu_seconds / 4))
+            per_step.append((rate, n, wall))
+        timed = per_step[args.warmup:]
+        tot_n = sum(x[1] for x in timed)
+        tot_t = sum(x[2] for x in timed)
+        value = tot_n / tot_t
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "magnifications/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config,
+            "cpu_baseline": {"value": value, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                             "sample": f"{tot_n} points of the batch over {args.steps} steps"},
+            "e2e": {"value": value, "unit": "magnifications/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+
+    import lcbinint_b200 as lb
+    from lcbinint_b200 import _lib
+    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, PS_EXACT, PS_ON_DEVICE, LcbiStructs
+
+    ctx = lb.context(local_rank)
+    L = ctx._L
+    stream = torch.cuda.current_stream(dev)
+    L.lcbi_gpu_set_stream(ctx.handle, stream.cuda_stream)
+
+    settings, sidx = fs_settings_for(rows)
+    st_arr = (LcbiStructs.FsSettings * len(settings))(*settings)
+    # models: distinct (s, q_core)
+    mkeys = {}
+    mlist = []
+    midx = np.empty(len(rows), dtype=np.int32)
+    for i, r in enumerate(rows):
+        k = (r[0], r[1])
+        if k not in mkeys:
+            mkeys[k] = len(mlist)
+            mlist.append((r[0], r[1], 1400, 0))
+        midx[i] = mkeys[k]
+    models = np.array(mlist, dtype=np.dtype([("s", "f8"), ("q", "f8"), ("bins", "i4"), ("r", "i4")]))
+    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
+    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
+    pts["settings"] = sidx
+    pts["model"] = midx
+    pts["flags"] = PS_EXACT | PS_ON_DEVICE
+    n = len(pts)
+    d_pts = torch.from_numpy(pts.view(np.uint8).copy()).to(dev)
+    d_res = torch.zeros(n * FS_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step_device():
+        rc = L.lcbi_gpu_binary_mag(ctx.handle, st_arr, len(settings), models.ctypes.data, len(models), n,
+                                   d_pts.data_ptr(), d_res.data_ptr(), _lib.DEVICE_POINTERS | 2)
+        ctx.check(rc, "lcbi_gpu_binary_mag")
+
+    res_host = np.zeros(n, dtype=FS_RESULT_DTYPE)
+
+    def step_e2e():
+        rc = L.lcbi_gpu_binary_mag(ctx.handle, st_arr, len(settings), None, 0, n, pts.ctypes.data,
+                                   res_host.ctypes.data, 0)
+        ctx.check(rc, "lcbi_gpu_binary_mag")
+
+    for _ in range(args.warmup):
+        flush_l2(flush)
+        step_device()
+    torch.cuda.synchronize(dev)
+    launches0 = ctx.launches
+    L.lcbi_gpu_set_timing(ctx.handle, 1)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush_l2(flush)
+            ev0[k].record(stream)
+            step_device()
+            ev1[k].record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    my_ms = float(np.sum(step_ms))
+    launches = ctx.launches - launches0
+    stage_ms = np.zeros(8)
+    stage_n = np.zeros(8, dtype=np.int64)
+    L.lcbi_gpu_stage_times(ctx.handle, _lib.ptr(stage_ms), _lib.ptr(stage_n), 8)
+    L.lcbi_gpu_set_timing(ctx.handle, 0)
+    rays = np.zeros(n, dtype=np.uint64)
+    L.lcbi_gpu_last_ray_counts(ctx.handle, n, _lib.ptr(rays))
+    res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=FS_RESULT_DTYPE)
+    if world > 1:
+        t = torch.tensor([my_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        max_ms = float(t.item())
+    else:
+        max_ms = my_ms
+    ms_per_step = max_ms / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+
+    # end to end: host arrays through the public C ABI (planning, H2D copies,
+    # kernels, D2H of the results), wall-clocked per step
+    for _ in range(2):
+        step_e2e()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        step_e2e()
+        e2e_s += time.perf_counter() - t1
+
+    peak = ctypes_double()
+    L.lcbi_gpu_measure_fp64_peak(ctx.handle, peak.ref())
+    names = ["caustics+ld", "decide", "seeds", "cartesian", "polar", "point_source"]
+    shares = {names[i]: float(stage_ms[i]) for i in range(6)}
+    dom = int(np.argmax(stage_ms[:5]))
+    cart = res["method"] == 2
+    polar_m = res["method"] == 3
+    rays_cart = float(rays[cart].sum())
+    rays_polar = float(rays[polar_m].sum())
+    rays_total = float(rays.sum())
+    if dom in (3, 4):
+        dom_rays = rays_cart if dom == 3 else rays_polar
+        achieved = dom_rays * args.steps * F_RAY / (stage_ms[dom] * 1e-3) / 1e12
+    else:
+        achieved = None
+    roofline = {"bound": "fp64", "kernel": names[dom], "achieved": achieved, "peak": peak.value,
+                "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved and peak.value else None,
+                "traffic": None, "peak_source": "device-measured FP64 FMA loop (lcbi_gpu_measure_fp64_peak)",
+                "stage_ms_per_step": {k: v / args.steps for k, v in shares.items()},
+                "flop_per_ray": F_RAY}
+    out = {
+        "metric": METRIC, "value": value, "unit": "magnifications/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+        "rays_per_s": world * rays_total / (ms_per_step * 1e-3),
+        "methods": {"cartesian": int(cart.sum()), "polar": int(polar_m.sum())},
+        "status_ok": int((res["status"] == 0).sum()),
+        "roofline": roofline,
+        "e2e": {"value": n * args.steps / e2e_s, "unit": "magnifications/s",
+                "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(res_host.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, nn, wall = cpu_reference_rate(rows, ncores, target_seconds=args.cpu_seconds)
+        out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                               "sample": f"{nn} random points of the batch, {wall:.1f} s wall on {ncores} processes"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+class ctypes_double:
+    def __init__(self):
+        import ctypes
+        self._v = ctypes.c_double(0.0)
+
+    def ref(self):
+        import ctypes
+        return ctypes.byref(self._v)
+
+    @property
+    def value(self):
+        return self._v.value
+
+
+if __name__ == "__main__":
+    main()

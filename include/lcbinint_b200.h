@@ -47,6 +47,18 @@ void lcbi_gpu_destroy(lcbi_gpu_context *ctx);
 const char *lcbi_gpu_last_error(const lcbi_gpu_context *ctx);
 /* Number of kernels this context has launched (instrumentation). */
 int64_t lcbi_gpu_launch_count(const lcbi_gpu_context *ctx);
+/* Runs the context's work on a caller's cudaStream_t (NULL: the context's own
+ * stream), so callers can order and time it with their own events. */
+int lcbi_gpu_set_stream(lcbi_gpu_context *ctx, void *cuda_stream);
+/* Enables (and resets) per-stage kernel timing with CUDA events. */
+int lcbi_gpu_set_timing(lcbi_gpu_context *ctx, int enable);
+/* Accumulated device milliseconds and launch counts per stage since timing was
+ * enabled: 0 caustics + limb-darkening tables, 1 decision, 2 seeding,
+ * 3 Cartesian inverse ray, 4 polar inverse ray, 5 point source. */
+int lcbi_gpu_stage_times(const lcbi_gpu_context *ctx, double *ms, int64_t *launches, int32_t n);
+/* Device-measured FP64 fused-multiply-add throughput of this GPU in TFLOP/s
+ * (2 flop per FMA), the denominator of the FP64 roofline; no reference counterpart. */
+int lcbi_gpu_measure_fp64_peak(lcbi_gpu_context *ctx, double *tflops);
 
 /* Point-source magnification of n source positions.
  * Replaces PointSourceMagnifier::binary_mag0
@@ -68,6 +80,104 @@ int lcbi_gpu_binary_mag0_derivatives(lcbi_gpu_context *ctx, int64_t n, const dou
                                      const double *q, const double *y1, const double *y2,
                                      double *A, int32_t *image_count, double *indicator,
                                      unsigned flags);
+
+/* ------------------------------------------------------------------ */
+/* Finite source                                                       */
+/* ------------------------------------------------------------------ */
+
+/* FiniteSourceSettings (src/lcbinint/magnification/finite_source_magnifier.hpp:22-38). */
+typedef struct lcbi_fs_settings {
+    int32_t source_bins;             /* nbin: cells per source radius */
+    int32_t caustic_bins;            /* caustic phase samples (>= 32 used) */
+    double grid_ratio;
+    int32_t polar_source_bins;       /* 0: use source_bins */
+    double polar_grid_ratio;         /* <= 0: use grid_ratio */
+    int32_t finite_mode;             /* 1 cartesian, 2 polar, 4 auto */
+    double kinji_threshold;          /* bounding-box margin for the point-source exit, in rho */
+    double hex_threshold;            /* caustic-distance threshold, in rho */
+    double adaptive_hex_threshold;   /* hexadecapole tolerance */
+    double limb_darkening_c;
+    double limb_darkening_d;
+    int32_t adaptive_source_bins;    /* must be 0: local adaptive refinement is not implemented */
+    int32_t max_source_bins;
+    double finite_source_tol;
+    double finite_source_reltol;
+} lcbi_fs_settings;
+
+/* One evaluation of FiniteSourceMagnifier::binary_mag
+ * (src/lcbinint/magnification/finite_source_magnifier.cpp:4633-4642):
+ * core convention (q < 1: heavier lens at -s; q > 1 inverted), source (y1, y2)
+ * in the centre-of-mass frame, radius rho. */
+typedef struct lcbi_fs_point {
+    double s, q, y1, y2, rho;
+    double point_source_magnification;  /* ignored with LCBI_FS_PS_ON_DEVICE */
+    int32_t settings;                   /* index into the settings table */
+    int32_t model;                      /* index into the lens-model table (LCBI_GPU_MODELS_GIVEN) */
+    int32_t flags;                      /* LCBI_FS_PS_EXACT | LCBI_FS_PS_ON_DEVICE */
+    int32_t reserved;
+} lcbi_fs_point;
+
+#define LCBI_FS_PS_EXACT 1      /* point_source_magnification_is_exact */
+#define LCBI_FS_PS_ON_DEVICE 2  /* point_source_magnification = binary_mag0(s, q, y1, y2), on the GPU */
+
+/* A caustic model (s, q, caustic_bins), the key of the reference's caustic
+ * cache (finite_source_magnifier.cpp:4014-4022). */
+typedef struct lcbi_lens_model {
+    double s, q;
+    int32_t caustic_bins;
+    int32_t reserved;
+} lcbi_lens_model;
+
+/* FiniteSourceResult (finite_source_magnifier.hpp:53-60). */
+typedef struct lcbi_fs_result {
+    double magnification;
+    double error_estimate;
+    int32_t method;       /* 0 point source, 1 hexadecapole, 2 Cartesian, 3 polar */
+    int32_t converged;
+    int32_t status;       /* LCBI_OK, LCBI_NUMERICAL_ERROR, or LCBI_GPU_LIMIT_* */
+    int32_t seed_count;   /* inverse-ray image seeds used */
+} lcbi_fs_result;
+
+/* Per-item device limits (the item's magnification is NaN). */
+#define LCBI_GPU_LIMIT_SEEDS 17
+#define LCBI_GPU_LIMIT_ROWS 18
+#define LCBI_GPU_LIMIT_QUEUE 19
+
+#define LCBI_GPU_MODELS_GIVEN 2u  /* points carry model indices into `models` */
+
+/* Finite-source magnification of n points in one batched launch sequence.
+ * Replaces FiniteSourceMagnifier::binary_mag
+ * (src/lcbinint/magnification/finite_source_magnifier.cpp:4633-4843): the same
+ * decision tree (caustic bounding box, derivative check, hexadecapole,
+ * Cartesian or polar inverse ray) evaluated per point.  `settings` and
+ * `models` are host arrays; without LCBI_GPU_MODELS_GIVEN the library derives
+ * the models from the points (host `points` required).  Returns LCBI_OK when
+ * the batch ran; per-point failures are in results[i].status. */
+int lcbi_gpu_binary_mag(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_settings,
+                        const lcbi_lens_model *models, int32_t n_models, int64_t n,
+                        const lcbi_fs_point *points, lcbi_fs_result *results, unsigned flags);
+
+/* lcbinint.binary_inverse_ray over n source positions
+ * (python/lcbinint_pybind.cpp:3826-3847): the decision thresholds are forced
+ * (kinji_threshold 1e18, hex thresholds 0) so every point is integrated by
+ * inverse ray; q is passed to the core unchanged.  Host arrays only. */
+int lcbi_gpu_binary_inverse_ray(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int64_t n,
+                                const double *s, const double *q, const double *y1, const double *y2,
+                                const double *rho, double *A, int32_t *method, int32_t *status);
+
+/* Static binary light curves, VBM convention: the fast path of
+ * lcbinint.LightCurve.__call__ (python/lcbinint_pybind.cpp:1087-1174).
+ * params[m] = {t0, tE, u0, alpha, s, q, rho} (q in VBM convention, inverted
+ * internally); times[first[m] .. first[m]+count[m]) are model m's epochs.
+ * Host arrays only; A has one value per epoch. */
+int lcbi_gpu_light_curves(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_models,
+                          const double *params, const int64_t *first, const int32_t *count,
+                          const double *times, int64_t n_times, double *A, int32_t *method, int32_t *status);
+
+/* Lattice cells counted by the last finite-source call (one count per point,
+ * cells whose centre maps inside the source disk), for ray-throughput
+ * accounting; no reference counterpart.  n must not exceed that call's size. */
+int lcbi_gpu_last_ray_counts(lcbi_gpu_context *ctx, int64_t n, uint64_t *rays);
 
 #ifdef __cplusplus
 }

@@ -11,10 +11,25 @@ import numpy as np
 
 from . import _lib
 from ._lib import GpuError, LibraryMissing, context
+from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, LightCurve, LightCurveFunc, LightCurveInfo,
+                  LimbDarkening, Options, binary_inverse_ray, binary_inverse_ray_batch, binary_mag, light_curves)
 
 __all__ = [
     "binary_mag0",
     "binary_mag0_batch",
+    "binary_inverse_ray",
+    "binary_inverse_ray_batch",
+    "binary_mag",
+    "light_curves",
+    "LightCurve",
+    "LightCurveFunc",
+    "LightCurveInfo",
+    "LimbDarkening",
+    "Options",
+    "EventCoordinates",
+    "STATIC",
+    "CIRCULAR",
+    "KEPLER",
     "GpuError",
     "LibraryMissing",
     "context",

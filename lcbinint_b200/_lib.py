@@ -62,6 +62,22 @@ def _declare(L):
     L.lcbi_gpu_binary_mag0_derivatives.argtypes = [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                                    C.c_uint]
     L.lcbi_gpu_binary_mag0_derivatives.restype = C.c_int
+    L.lcbi_gpu_binary_mag.argtypes = [_vp, _vp, C.c_int32, _vp, C.c_int32, C.c_int64, _vp, _vp, C.c_uint]
+    L.lcbi_gpu_binary_mag.restype = C.c_int
+    L.lcbi_gpu_binary_inverse_ray.argtypes = [_vp, _vp, C.c_int64] + [_vp] * 8
+    L.lcbi_gpu_binary_inverse_ray.restype = C.c_int
+    L.lcbi_gpu_light_curves.argtypes = [_vp, _vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp, _vp]
+    L.lcbi_gpu_light_curves.restype = C.c_int
+    L.lcbi_gpu_set_stream.argtypes = [_vp, _vp]
+    L.lcbi_gpu_set_stream.restype = C.c_int
+    L.lcbi_gpu_set_timing.argtypes = [_vp, C.c_int]
+    L.lcbi_gpu_set_timing.restype = C.c_int
+    L.lcbi_gpu_stage_times.argtypes = [_vp, _vp, _vp, C.c_int32]
+    L.lcbi_gpu_stage_times.restype = C.c_int
+    L.lcbi_gpu_measure_fp64_peak.argtypes = [_vp, _vp]
+    L.lcbi_gpu_measure_fp64_peak.restype = C.c_int
+    L.lcbi_gpu_last_ray_counts.argtypes = [_vp, C.c_int64, _vp]
+    L.lcbi_gpu_last_ray_counts.restype = C.c_int
 
 
 def exported_symbols() -> list[str]:

@@ -1,0 +1,423 @@
+"""Python mirror of the reference's pybind11 API for the magnification path.
+
+Names, argument names, defaults and error behaviour follow
+python/lcbinint_pybind.cpp (Options :2985-3112, LimbDarkening :2828-2846,
+LightCurve :3114-3406, binary_mag0 :3819-3824, binary_inverse_ray :3826-3847).
+Every computation is a call into the C ABI of the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import context
+
+
+class LcbiStructs:
+    class FsSettings(C.Structure):
+        _fields_ = [
+            ("source_bins", C.c_int32), ("caustic_bins", C.c_int32), ("grid_ratio", C.c_double),
+            ("polar_source_bins", C.c_int32), ("polar_grid_ratio", C.c_double), ("finite_mode", C.c_int32),
+            ("kinji_threshold", C.c_double), ("hex_threshold", C.c_double),
+            ("adaptive_hex_threshold", C.c_double), ("limb_darkening_c", C.c_double),
+            ("limb_darkening_d", C.c_double), ("adaptive_source_bins", C.c_int32),
+            ("max_source_bins", C.c_int32), ("finite_source_tol", C.c_double),
+            ("finite_source_reltol", C.c_double),
+        ]
+
+    class FsPoint(C.Structure):
+        _fields_ = [("s", C.c_double), ("q", C.c_double), ("y1", C.c_double), ("y2", C.c_double),
+                    ("rho", C.c_double), ("point_source_magnification", C.c_double),
+                    ("settings", C.c_int32), ("model", C.c_int32), ("flags", C.c_int32),
+                    ("reserved", C.c_int32)]
+
+    class FsResult(C.Structure):
+        _fields_ = [("magnification", C.c_double), ("error_estimate", C.c_double), ("method", C.c_int32),
+                    ("converged", C.c_int32), ("status", C.c_int32), ("seed_count", C.c_int32)]
+
+
+FS_POINT_DTYPE = np.dtype([("s", "f8"), ("q", "f8"), ("y1", "f8"), ("y2", "f8"), ("rho", "f8"),
+                           ("a_ps", "f8"), ("settings", "i4"), ("model", "i4"), ("flags", "i4"),
+                           ("reserved", "i4")])
+FS_RESULT_DTYPE = np.dtype([("magnification", "f8"), ("error_estimate", "f8"), ("method", "i4"),
+                            ("converged", "i4"), ("status", "i4"), ("seed_count", "i4")])
+PS_EXACT = 1
+PS_ON_DEVICE = 2
+METHOD_NAMES = {0: "point_source", 1: "hexadecapole", 2: "inverse_ray_cartesian", 3: "inverse_ray_polar",
+                4: "inverse_ray_spine", 5: "source_plane_quadrature"}
+
+
+@dataclass
+class LimbDarkening:
+    """Source surface brightness I = 1 - c(1 - mu) - d(1 - sqrt(mu)) (PYB:2828-2846)."""
+
+    c: float = 0.0
+    d: float = 0.0
+
+    @staticmethod
+    def none() -> "LimbDarkening":
+        return LimbDarkening()
+
+    @staticmethod
+    def linear(c: float) -> "LimbDarkening":
+        return LimbDarkening(float(c), 0.0)
+
+    @staticmethod
+    def quadratic(c: float, d: float) -> "LimbDarkening":
+        return LimbDarkening(float(c), float(d))
+
+    def __repr__(self):
+        return f"LimbDarkening(c={self.c:.6f}, d={self.d:.6f})"
+
+
+@dataclass
+class EventCoordinates:
+    ra: float = 0.0
+    dec: float = 0.0
+    tfix: float = 0.0
+    obs_lat: float = 0.0
+    obs_lon: float = 0.0
+
+
+_GRID_MODE = {"auto": 4, "": 4, "cartesian": 1, "inverse_ray_cartesian": 1, "polar": 2, "inverse_ray_polar": 2}
+_GRID_NAME = {4: "auto", 1: "cartesian", 2: "polar"}
+
+
+def _apply_param_type(o: "Options", name: str):
+    # apply_param_type (PYB:246-276)
+    if name in ("auto", "", "vbm", "vbbl", "standard"):
+        o.center_of_mass, o.vbm_compatible = 0, 1
+    elif name in ("lcbinint", "original", "legacy"):
+        o.center_of_mass, o.vbm_compatible = 0, 0
+    elif name == "center_of_mass":
+        o.center_of_mass, o.vbm_compatible = 1, 0
+    elif name == "vbm_center_of_mass":
+        o.center_of_mass, o.vbm_compatible = 1, 1
+    else:
+        raise ValueError("param_type must be 'vbm', 'lcbinint', 'original', or 'center_of_mass'")
+
+
+class Options:
+    """Computation options; defaults and aliases of lcbinint.Options (PYB:2985-3112)."""
+
+    def __init__(self, source_bins: int = 50, nbin=None, inverse_ray_grid: str = "auto",
+                 caustic_bins: int = 1400, grid_ratio: float = 4.0, polar_nbin=None, polar_source_bins=None,
+                 polar_grid_ratio=None, point_source_threshold: float = 20.0,
+                 hexadecapole_threshold: float = 3.0, adaptive_hex_threshold: float = 0.001,
+                 adaptive_source_bins: int = -1, max_source_bins: int = 400, finite_source_tol: float = 0.0,
+                 finite_source_reltol: float = 0.0, tol: float = math.nan, reltol: float = math.nan,
+                 coordinates: str = "auto", hex_tol: float = math.nan, param_type: str = "auto",
+                 xallarap_param_type: str = "none"):
+        self.center_of_mass, self.vbm_compatible = 0, 1
+        if param_type and param_type != "auto":
+            _apply_param_type(self, param_type)
+        else:
+            _apply_param_type(self, coordinates)
+        if xallarap_param_type not in ("", "none", "angular_velocity", "orbital_elements"):
+            raise ValueError("xallarap_param_type must be 'none', 'angular_velocity', or 'orbital_elements'")
+        self._xallarap = xallarap_param_type or "none"
+        self.inverse_ray_grid = inverse_ray_grid
+        self.source_bins = int(source_bins if nbin is None else nbin)
+        self.caustic_bins = int(caustic_bins)
+        self.grid_ratio = float(grid_ratio)
+        pn = polar_nbin if polar_nbin is not None else polar_source_bins
+        self.polar_source_bins = int(pn) if pn is not None else 0
+        self._polar_grid_ratio = float(polar_grid_ratio) if polar_grid_ratio is not None else 0.0
+        self.point_source_threshold = float(point_source_threshold)
+        self.hexadecapole_threshold = float(hexadecapole_threshold)
+        self.adaptive_hex_threshold = float(adaptive_hex_threshold if math.isnan(hex_tol) else hex_tol)
+        self.max_source_bins = int(max_source_bins)
+        self.finite_source_tol = float(finite_source_tol if math.isnan(tol) else tol)
+        self.finite_source_reltol = float(finite_source_reltol if math.isnan(reltol) else reltol)
+        self.adaptive_source_bins = 0 if adaptive_source_bins < 0 else int(adaptive_source_bins)
+
+    # ---- properties with the reference's aliases ----
+    @property
+    def nbin(self) -> int:
+        return self.source_bins
+
+    @nbin.setter
+    def nbin(self, v: int):
+        self.source_bins = int(v)
+
+    @property
+    def inverse_ray_grid(self) -> str:
+        return _GRID_NAME.get(self._mode, "internal")
+
+    @inverse_ray_grid.setter
+    def inverse_ray_grid(self, v: str):
+        if v not in _GRID_MODE:
+            raise ValueError("inverse_ray_grid must be 'auto', 'cartesian', or 'polar'")
+        self._mode = _GRID_MODE[v]
+
+    @property
+    def polar_nbin(self):
+        return self.polar_source_bins if self.polar_source_bins > 0 else None
+
+    @polar_nbin.setter
+    def polar_nbin(self, v):
+        self.polar_source_bins = 0 if v is None else int(v)
+
+    @property
+    def polar_grid_ratio(self):
+        return self._polar_grid_ratio if self._polar_grid_ratio > 0 else None
+
+    @polar_grid_ratio.setter
+    def polar_grid_ratio(self, v):
+        self._polar_grid_ratio = 0.0 if v is None else float(v)
+
+    @property
+    def hex_tol(self) -> float:
+        return self.adaptive_hex_threshold
+
+    @hex_tol.setter
+    def hex_tol(self, v):
+        self.adaptive_hex_threshold = float(v)
+
+    @property
+    def tol(self) -> float:
+        return self.finite_source_tol
+
+    @tol.setter
+    def tol(self, v):
+        self.finite_source_tol = float(v)
+
+    @property
+    def reltol(self) -> float:
+        return self.finite_source_reltol
+
+    @reltol.setter
+    def reltol(self, v):
+        self.finite_source_reltol = float(v)
+
+    @property
+    def coordinates(self) -> str:
+        if self.vbm_compatible and not self.center_of_mass:
+            return "vbm"
+        if self.center_of_mass and self.vbm_compatible:
+            return "vbm_center_of_mass"
+        if self.center_of_mass:
+            return "center_of_mass"
+        return "lcbinint"
+
+    @coordinates.setter
+    def coordinates(self, v: str):
+        _apply_param_type(self, v)
+
+    param_type = coordinates
+
+    @property
+    def xallarap_param_type(self) -> str:
+        return self._xallarap
+
+    def fs_settings(self, ld: LimbDarkening) -> LcbiStructs.FsSettings:
+        """make_finite_source_settings (PYB:471-492)."""
+        return LcbiStructs.FsSettings(
+            source_bins=self.source_bins, caustic_bins=self.caustic_bins, grid_ratio=self.grid_ratio,
+            polar_source_bins=self.polar_source_bins, polar_grid_ratio=self._polar_grid_ratio,
+            finite_mode=self._mode, kinji_threshold=self.point_source_threshold,
+            hex_threshold=self.hexadecapole_threshold, adaptive_hex_threshold=self.adaptive_hex_threshold,
+            limb_darkening_c=ld.c, limb_darkening_d=ld.d, adaptive_source_bins=self.adaptive_source_bins,
+            max_source_bins=self.max_source_bins, finite_source_tol=self.finite_source_tol,
+            finite_source_reltol=self.finite_source_reltol)
+
+
+def _raise_for_status(status, what="numerical error"):
+    status = np.asarray(status)
+    bad = status != _lib.LCBI_OK
+    if bad.any():
+        code = int(status[bad][0])
+        if code == _lib.LCBI_NUMERICAL_ERROR:
+            raise RuntimeError("numerical error")
+        if code == _lib.LCBI_UNSUPPORTED:
+            raise RuntimeError("unsupported")
+        raise RuntimeError(f"{what}: device limit reached (status {code})")
+
+
+def binary_mag(points, settings_list, *, device: int = 0, models=None):
+    """Batched FiniteSourceMagnifier::binary_mag over a structured array of
+    FS_POINT_DTYPE records; returns a FS_RESULT_DTYPE array."""
+    pts = np.ascontiguousarray(points, dtype=FS_POINT_DTYPE)
+    n = pts.size
+    res = np.zeros(n, dtype=FS_RESULT_DTYPE)
+    if n == 0:
+        return res
+    st = (LcbiStructs.FsSettings * len(settings_list))(*settings_list)
+    ctx = context(device)
+    flags = 0
+    mptr, nm = None, 0
+    if models is not None:
+        md = np.ascontiguousarray(models, dtype=np.dtype([("s", "f8"), ("q", "f8"), ("bins", "i4"),
+                                                             ("r", "i4")]))
+        mptr, nm = md.ctypes.data, md.size
+        flags |= 2
+    rc = ctx._L.lcbi_gpu_binary_mag(ctx.handle, st, len(settings_list), mptr, nm, n, pts.ctypes.data,
+                                    res.ctypes.data, flags)
+    ctx.check(rc, "lcbi_gpu_binary_mag")
+    return res
+
+
+def binary_inverse_ray_batch(s, q, x, y, rho, limb_darkening: LimbDarkening = None, options: Options = None,
+                             *, device: int = 0, return_method: bool = False):
+    """Batched lcbinint.binary_inverse_ray: the same forced inverse-ray decision
+    per point (PYB:3826-3847), all points in one launch sequence."""
+    ld = limb_darkening or LimbDarkening()
+    opt = options or Options()
+    arrs = np.broadcast_arrays(s, q, x, y, rho)
+    shape = arrs[0].shape
+    s, q, x, y, rho = (_lib.as_f64(a) for a in arrs)
+    n = s.size
+    A = np.empty(n)
+    method = np.empty(n, dtype=np.int32)
+    status = np.empty(n, dtype=np.int32)
+    st = opt.fs_settings(ld)
+    ctx = context(device)
+    rc = ctx._L.lcbi_gpu_binary_inverse_ray(ctx.handle, C.byref(st), n, _lib.ptr(s), _lib.ptr(q), _lib.ptr(x),
+                                            _lib.ptr(y), _lib.ptr(rho), _lib.ptr(A), _lib.ptr(method),
+                                            _lib.ptr(status))
+    ctx.check(rc, "lcbi_gpu_binary_inverse_ray")
+    if return_method:
+        return A.reshape(shape), method.reshape(shape), status.reshape(shape)
+    return A.reshape(shape)
+
+
+def binary_inverse_ray(s: float, q: float, x: float, y: float, rho: float,
+                       limb_darkening: LimbDarkening = None, options: Options = None) -> float:
+    """Binary finite-source magnification at (x, y) by inverse-ray shooting,
+    same convention as VBMicrolensing BinaryMag2 (PYB:3826-3847)."""
+    return float(binary_inverse_ray_batch(s, q, x, y, rho, limb_darkening, options).reshape(-1)[0])
+
+
+def light_curves(times_list, params_list, options: Options = None, limb_darkening: LimbDarkening = None,
+                 *, device: int = 0, return_method: bool = False):
+    """Many static binary light curves (VBM convention) in one batched launch.
+
+    times_list[m] are model m's epochs; params_list[m] is a dict with t0, tE,
+    u0, alpha, s, q, rho.  Returns a list of arrays."""
+    opt = options or Options()
+    ld = limb_darkening or LimbDarkening()
+    nm = len(params_list)
+    counts = np.array([len(t) for t in times_list], dtype=np.int32)
+    first = np.zeros(nm, dtype=np.int64)
+    if nm > 1:
+        first[1:] = np.cumsum(counts[:-1])
+    times = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64).ravel() for t in times_list])
+                                 if nm else np.zeros(0))
+    P = np.array([[p.get("t0", 0.0), p.get("tE", 1.0), p.get("u0", 0.0), p.get("alpha", 0.0),
+                   p.get("s", 1.0), p.get("q", 1.0), p.get("rho", 0.0)] for p in params_list],
+                 dtype=np.float64).reshape(nm, 7)
+    n = times.size
+    A = np.empty(n)
+    method = np.empty(n, dtype=np.int32)
+    status = np.empty(n, dtype=np.int32)
+    st = opt.fs_settings(ld)
+    ctx = context(device)
+    rc = ctx._L.lcbi_gpu_light_curves(ctx.handle, C.byref(st), nm, _lib.ptr(P), _lib.ptr(first), _lib.ptr(counts),
+                                      _lib.ptr(times), n, _lib.ptr(A), _lib.ptr(method), _lib.ptr(status))
+    ctx.check(rc, "lcbi_gpu_light_curves")
+    out = np.split(A, np.cumsum(counts)[:-1]) if nm else []
+    if return_method:
+        return out, np.split(method, np.cumsum(counts)[:-1]), np.split(status, np.cumsum(counts)[:-1])
+    return out
+
+
+STATIC = 0
+CIRCULAR = 1
+KEPLER = 2
+
+
+class LightCurve:
+    """lcbinint.LightCurve (PYB:3114-3406): a reusable light-curve callable.
+
+    The static binary lens in VBM coordinates (the reference's direct fast
+    path, PYB:1087-1174) and binary sources (PYB:2331-2354) run on the GPU.
+    Orbital motion, parallax and the original/centre-of-mass conventions are
+    not implemented and raise NotImplementedError."""
+
+    def __init__(self, *, lens: str = "binary_lens", source: str = "single", event: EventCoordinates = None,
+                 options: Options = None, limb_darkening: LimbDarkening = None, orbital_motion_mode: int = STATIC,
+                 parallax: bool = False, terrestrial_parallax: bool = False):
+        if lens not in ("binary_lens", "binary", "binary-lens", ""):
+            if lens in ("triple_lens", "triple"):
+                raise NotImplementedError("triple lenses are outside this implementation")
+            raise ValueError("lens must be 'binary_lens' or 'triple_lens'")
+        if source in ("", "single"):
+            source = "single"
+        elif source in ("binary", "binary_source"):
+            source = "binary"
+        else:
+            raise ValueError("source must be 'single' or 'binary'")
+        self.lens = "binary_lens"
+        self.source = source
+        self.event = event or EventCoordinates()
+        self.options = options or Options()
+        self.limb_darkening = limb_darkening or LimbDarkening()
+        self.orbital_motion_mode = orbital_motion_mode
+        self.parallax = parallax
+        self.terrestrial_parallax = terrestrial_parallax
+
+    def _check_supported(self, p):
+        if self.orbital_motion_mode != STATIC or self.parallax or self.terrestrial_parallax:
+            raise NotImplementedError("orbital motion and parallax are not implemented on the GPU path")
+        if not (self.options.vbm_compatible and not self.options.center_of_mass):
+            raise NotImplementedError("only the 'vbm' coordinate convention is implemented")
+        for k in ("piEN", "piEE", "xi_1", "xi_2", "piEN_xa", "piEE_xa"):
+            if p.get(k, 0.0) != 0.0:
+                raise NotImplementedError(f"{k} != 0 is not implemented on the GPU path")
+
+    def _single(self, times, p):
+        self._check_supported(p)
+        (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
+        _raise_for_status(st)
+        return A
+
+    def __call__(self, times, params=None, **kw):
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        if times.ndim != 1:
+            raise ValueError("times must be one-dimensional")
+        p = dict(params) if params is not None else {}
+        p.update(kw)
+        if self.source == "binary":
+            p2 = dict(p)
+            p2["u0"] = p.get("u0_2", 0.0)
+            p2["t0"] = p.get("t0_2", 0.0)
+            v1 = self._single(times, p)
+            v2 = self._single(times, p2)
+            fr = p.get("flux_ratio", 0.0)
+            inv = 1.0 / (1.0 + fr)
+            return (v1 + fr * v2) * inv
+        return self._single(times, p)
+
+    light_curve = __call__
+
+    def list(self, times, **kw):
+        return [float(v) for v in self(np.asarray(times, dtype=np.float64), **kw)]
+
+    def magnification(self, time, params=None, **kw):
+        return float(self(np.array([float(time)]), params, **kw)[0])
+
+    def info(self, times, params=None, **kw):
+        """Per-epoch magnifications with the finite-source method chosen."""
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        p = dict(params) if params is not None else {}
+        p.update(kw)
+        self._check_supported(p)
+        (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
+        _raise_for_status(st)
+        return LightCurveInfo(times=list(times), magnifications=list(A), finite_source_methods=list(m),
+                              finite_source_method_names=[METHOD_NAMES[int(v)] for v in m])
+
+
+@dataclass
+class LightCurveInfo:
+    times: list = field(default_factory=list)
+    magnifications: list = field(default_factory=list)
+    finite_source_methods: list = field(default_factory=list)
+    finite_source_method_names: list = field(default_factory=list)
+
+
+LightCurveFunc = LightCurve

@@ -53,7 +53,56 @@ Context::~Context()
     for (Buffer* b : all_buffers()) {
         if (b->ptr) cudaFree(b->ptr);
     }
-    if (stream) cudaStreamDestroy(stream);
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    for (auto& p : pending) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+void Context::stage_begin(int stage, cudaEvent_t* ev)
+{
+    (void)stage;
+    *ev = nullptr;
+    if (!timing) return;
+    if (event_pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        event_pool.push_back(e);
+    }
+    *ev = event_pool.back();
+    event_pool.pop_back();
+    cudaEventRecord(*ev, stream);
+}
+
+void Context::stage_end(int stage, cudaEvent_t begin)
+{
+    if (!timing || begin == nullptr) return;
+    cudaEvent_t e;
+    if (event_pool.empty()) {
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+    } else {
+        e = event_pool.back();
+        event_pool.pop_back();
+    }
+    cudaEventRecord(e, stream);
+    pending.push_back({stage, {begin, e}});
+}
+
+void Context::collect_timing()
+{
+    for (auto& p : pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess && p.first >= 0 &&
+            p.first < kStages) {
+            stage_ms[p.first] += ms;
+            stage_launches[p.first] += 1;
+        }
+        event_pool.push_back(p.second.first);
+        event_pool.push_back(p.second.second);
+    }
+    pending.clear();
 }
 
 // Stages `count` elements of an input array: device pointers pass through,
@@ -94,7 +143,9 @@ bool Context::copy_back(T* dst, const T* dev, size_t count, bool device_ptrs)
 
 bool Context::finish()
 {
-    return check("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+    const bool ok = check("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+    if (ok) collect_timing();
+    return ok;
 }
 
 template bool Context::stage_in<double>(Buffer&, const double*, size_t, bool, const double**);
@@ -121,13 +172,45 @@ int lcbi_gpu_create(int device, lcbi_gpu_context** out)
     if (!ctx) return LCBI_GPU_ERROR;
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
         return LCBI_GPU_ERROR;
     }
+    ctx->stream = ctx->own_stream;
     *out = reinterpret_cast<lcbi_gpu_context*>(ctx);
+    return LCBI_OK;
+}
+
+int lcbi_gpu_set_stream(lcbi_gpu_context* c, void* stream)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_set_timing(lcbi_gpu_context* c, int enable)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->timing = enable != 0;
+    for (int i = 0; i < Context::kStages; ++i) {
+        ctx->stage_ms[i] = 0.0;
+        ctx->stage_launches[i] = 0;
+    }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_stage_times(const lcbi_gpu_context* c, double* ms, int64_t* launches, int32_t n)
+{
+    const Context* ctx = reinterpret_cast<const Context*>(c);
+    if (!ctx || !ms || n < 0) return LCBI_INVALID_ARGUMENT;
+    for (int i = 0; i < n && i < Context::kStages; ++i) {
+        ms[i] = ctx->stage_ms[i];
+        if (launches) launches[i] = ctx->stage_launches[i];
+    }
     return LCBI_OK;
 }
 
@@ -166,9 +249,12 @@ int lcbi_gpu_binary_mag0(lcbi_gpu_context* c, int64_t n, const double* s, const 
         !ctx->stage_out(ctx->out[1], reinterpret_cast<int*>(image_count), N, dev, &dn) ||
         !ctx->stage_out(ctx->out[2], reinterpret_cast<int*>(status), N, dev, &dst))
         return LCBI_GPU_ERROR;
+    cudaEvent_t t0;
+    ctx->stage_begin(5, &t0);
     if (!ctx->check("ps_batch_kernel", lcbi::launch_ps_batch(ds, dq, dy1, dy2, dA, dn, dst, n, ctx->sm_count,
                                                              ctx->stream)))
         return LCBI_GPU_ERROR;
+    ctx->stage_end(5, t0);
     ctx->launches += 1;
     if (!ctx->copy_back(A, dA, N, dev) || !ctx->copy_back(reinterpret_cast<int*>(image_count), dn, N, dev) ||
         !ctx->copy_back(reinterpret_cast<int*>(status), dst, N, dev) || !ctx->finish())

@@ -1,0 +1,520 @@
+// C-ABI host runtime of the finite-source pipeline:
+//   caustic models -> decision kernel -> seeding -> Cartesian / polar inverse ray.
+// The host only plans (de-duplicates lens models, builds constant angle tables
+// with the host C library) and launches; all physics runs in the kernels.
+#include "../../include/lcbinint_b200.h"
+#include "lcbi_context.h"
+#include "lcbi_fs_kernels.h"
+#include "lcbi_kernels.h"
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+using lcbi::Context;
+
+namespace lcbi {
+namespace {
+
+static_assert(sizeof(FsOut) == sizeof(lcbi_fs_result), "result layout");
+static_assert(sizeof(FsItem) == sizeof(lcbi_fs_point), "point layout");
+
+constexpr int kChunk = 16384;
+constexpr double kHostPi = 3.14159265358979323846;
+
+// Constant angle tables, evaluated exactly as the reference evaluates them.
+bool ensure_trig(Context* ctx)
+{
+    if (ctx->trig_ready) return true;
+    std::vector<double2> t;
+    t.reserve(1400 + 400 + 64 + 16);
+    const double phase_step = 2.0 * kHostPi / static_cast<double>(1400);
+    for (int k = 0; k < 1400; ++k) {
+        const std::complex<double> p = std::polar(1.0, phase_step * static_cast<double>(k));
+        t.push_back(make_double2(p.real(), p.imag()));
+    }
+    for (int i = 0; i < 400; ++i) {
+        const double phi = 2.0 * kHostPi * static_cast<double>(i) / static_cast<double>(400);
+        t.push_back(make_double2(std::cos(phi), std::sin(phi)));
+    }
+    for (int i = 0; i < 64; ++i) {
+        const double phi = 2.0 * kHostPi * static_cast<double>(i) / static_cast<double>(64);
+        t.push_back(make_double2(std::cos(phi), std::sin(phi)));
+    }
+    for (int i = 0; i < 16; ++i) {
+        const double th = 2.0 * kHostPi * static_cast<double>(i) / static_cast<double>(16);
+        t.push_back(make_double2(std::cos(th), std::sin(th)));
+    }
+    if (!ctx->ensure(ctx->fs_trig, t.size() * sizeof(double2))) return false;
+    if (!ctx->check("trig upload", cudaMemcpy(ctx->fs_trig.ptr, t.data(), t.size() * sizeof(double2),
+                                              cudaMemcpyHostToDevice)))
+        return false;
+    ctx->trig_ready = true;
+    return true;
+}
+
+TrigTables trig_of(Context* ctx)
+{
+    const double2* b = static_cast<const double2*>(ctx->fs_trig.ptr);
+    return TrigTables{b, b + 1400, b + 1800, b + 1864};
+}
+
+// Persistent-warp scratch, sized once per context and initialised to 0xff
+// (no generation tag matches it).
+bool ensure_scratch(Context* ctx)
+{
+    const int warps = ctx->sm_count * ctx->warps_per_sm;
+    if (ctx->fs_warps == warps) return true;
+    const size_t cart = (cartesian_scratch_bytes(ctx->row_cap, ctx->seed_cap) + 255) & ~size_t(255);
+    const size_t pol = (polar_scratch_bytes(ctx->queue_cap, ctx->hash_cap) + 255) & ~size_t(255);
+    if (!ctx->ensure(ctx->fs_scratch, cart * warps) || !ctx->ensure(ctx->fs_scratch_polar, pol * warps) ||
+        !ctx->ensure(ctx->fs_cand_keys, seed_candidate_bytes_per_warp() * warps))
+        return false;
+    if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart * warps, ctx->stream)) ||
+        !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff, pol * warps, ctx->stream)))
+        return false;
+    ctx->fs_warps = warps;
+    ctx->epoch = 0;
+    return true;
+}
+
+size_t cart_bytes_big(const Context* c) { return (cartesian_scratch_bytes(c->row_cap_big, c->seed_cap) + 255) & ~size_t(255); }
+size_t polar_bytes_big(const Context* c) { return (polar_scratch_bytes(c->queue_cap_big, c->hash_cap_big) + 255) & ~size_t(255); }
+
+bool ensure_big_scratch(Context* ctx)
+{
+    if (ctx->big_ready) return true;
+    const size_t cb = cart_bytes_big(ctx) * ctx->retry_warps;
+    const size_t pb = polar_bytes_big(ctx) * ctx->retry_warps;
+    if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb)) return false;
+    if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_big.ptr, 0xff, cb, ctx->stream)) ||
+        !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar_big.ptr, 0xff, pb, ctx->stream)))
+        return false;
+    ctx->big_ready = true;
+    return true;
+}
+
+FsSettingsDev to_dev(const lcbi_fs_settings& s, int ld_index)
+{
+    FsSettingsDev d;
+    d.source_bins = s.source_bins;
+    d.caustic_bins = s.caustic_bins;
+    d.grid_ratio = s.grid_ratio;
+    d.polar_source_bins = s.polar_source_bins;
+    d.polar_grid_ratio = s.polar_grid_ratio;
+    d.finite_mode = s.finite_mode;
+    d.kinji_threshold = s.kinji_threshold;
+    d.hex_threshold = s.hex_threshold;
+    d.adaptive_hex_threshold = s.adaptive_hex_threshold;
+    d.ld_c = s.limb_darkening_c;
+    d.ld_d = s.limb_darkening_d;
+    d.adaptive_source_bins = s.adaptive_source_bins;
+    d.max_source_bins = s.max_source_bins;
+    d.tol = s.finite_source_tol;
+    d.reltol = s.finite_source_reltol;
+    d.ld_table = ld_index;
+    d.pad = 0;
+    return d;
+}
+
+struct Plan {
+    std::vector<double2> ld_coeffs;  // distinct (c, d) pairs, one 20,001-entry table each
+    std::vector<FsSettingsDev> settings;
+    std::vector<CausticModel> models;
+    std::vector<long long> raw_offset;
+    std::vector<double2> phases;
+    int max_bins = 0;
+};
+
+// Adds the caustic model (s, q, max(bins, 32)) and its phase table; returns its index.
+struct ModelTable {
+    Plan* plan;
+    std::map<std::tuple<uint64_t, uint64_t, int>, int> index;
+    std::map<int, int> phase_offset;
+    long long raw_total = 0;
+
+    int get(double s, double q, int caustic_bins)
+    {
+        const int bins = caustic_bins > 32 ? caustic_bins : 32;
+        uint64_t bs, bq;
+        std::memcpy(&bs, &s, 8);
+        std::memcpy(&bq, &q, 8);
+        const auto key = std::make_tuple(bs, bq, bins);
+        auto it = index.find(key);
+        if (it != index.end()) return it->second;
+        auto po = phase_offset.find(bins);
+        int off;
+        if (po == phase_offset.end()) {
+            off = static_cast<int>(plan->phases.size());
+            for (int i = 0; i < bins; ++i) {
+                const double a = 2.0 * kHostPi * static_cast<double>(i) / static_cast<double>(bins);
+                const std::complex<double> p = std::polar(1.0, a);
+                plan->phases.push_back(make_double2(p.real(), p.imag()));
+            }
+            phase_offset[bins] = off;
+        } else {
+            off = po->second;
+        }
+        CausticModel m{};
+        m.s = s;
+        m.q = q;
+        m.bins = bins;
+        m.phase_offset = off;
+        m.branch_offset = raw_total;
+        plan->raw_offset.push_back(raw_total);
+        raw_total += 4ll * bins;
+        if (bins > plan->max_bins) plan->max_bins = bins;
+        const int id = static_cast<int>(plan->models.size());
+        plan->models.push_back(m);
+        index[key] = id;
+        return id;
+    }
+};
+
+// Adds settings with their limb-darkening table slot, sharing tables between
+// settings with the same (c, d).
+void add_settings(Plan& plan, const lcbi_fs_settings* s, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        int slot = -1;
+        for (size_t k = 0; k < plan.ld_coeffs.size(); ++k) {
+            if (plan.ld_coeffs[k].x == s[i].limb_darkening_c && plan.ld_coeffs[k].y == s[i].limb_darkening_d) {
+                slot = static_cast<int>(k);
+                break;
+            }
+        }
+        if (slot < 0) {
+            slot = static_cast<int>(plan.ld_coeffs.size());
+            plan.ld_coeffs.push_back(make_double2(s[i].limb_darkening_c, s[i].limb_darkening_d));
+        }
+        plan.settings.push_back(to_dev(s[i], slot));
+    }
+}
+
+template <typename T>
+bool upload(Context* ctx, Buffer& b, const std::vector<T>& v)
+{
+    if (!ctx->ensure(b, v.size() * sizeof(T) + 16)) return false;
+    if (v.empty()) return true;
+    return ctx->check("upload", cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                                ctx->stream));
+}
+
+// Runs the pipeline on device-resident items (ctx->fs_items) and writes device
+// results to ctx->fs_out.  Everything is asynchronous on ctx->stream.
+bool run_pipeline(Context* ctx, const Plan& plan, long long n)
+{
+    if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx)) return false;
+    const int nset = static_cast<int>(plan.settings.size());
+    const int nmod = static_cast<int>(plan.models.size());
+    const int nld = static_cast<int>(plan.ld_coeffs.size());
+    if (!upload(ctx, ctx->fs_settings, plan.settings) || !upload(ctx, ctx->fs_models, plan.models) ||
+        !upload(ctx, ctx->fs_raw_offset, plan.raw_offset) || !upload(ctx, ctx->fs_phases, plan.phases) ||
+        !upload(ctx, ctx->fs_ld_coeffs, plan.ld_coeffs))
+        return false;
+    long long raw_total = 0;
+    for (const auto& m : plan.models) raw_total += 4ll * m.bins;
+    if (!ctx->ensure(ctx->fs_raw, (raw_total + 1) * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_branches, (raw_total + 1) * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_ld, (size_t)(nld + 1) * (kLdTable + 1) * sizeof(double)) ||
+        !ctx->ensure(ctx->fs_rays, (size_t)(n + 1) * sizeof(unsigned long long)) ||
+        !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)))
+        return false;
+    (void)nset;
+    cudaEvent_t t0;
+    ctx->stage_begin(0, &t0);
+    if (!ctx->check("ld tables", launch_ld_tables(static_cast<double2*>(ctx->fs_ld_coeffs.ptr), nld,
+                                                  static_cast<double*>(ctx->fs_ld.ptr), ctx->stream)))
+        return false;
+    ctx->launches += 1;
+    if (!ctx->check("rays init", cudaMemsetAsync(ctx->fs_rays.ptr, 0, (size_t)n * sizeof(unsigned long long),
+                                                 ctx->stream)))
+        return false;
+    if (nmod > 0) {
+        if (!ctx->check("caustics", launch_caustics(static_cast<CausticModel*>(ctx->fs_models.ptr), nmod, plan.max_bins,
+                                                    static_cast<double2*>(ctx->fs_phases.ptr),
+                                                    static_cast<long long*>(ctx->fs_raw_offset.ptr),
+                                                    static_cast<P2*>(ctx->fs_raw.ptr), static_cast<P2*>(ctx->fs_branches.ptr),
+                                                    ctx->stream)))
+            return false;
+        ctx->launches += 2;
+    }
+    ctx->stage_end(0, t0);
+    const size_t cart_bytes = (cartesian_scratch_bytes(ctx->row_cap, ctx->seed_cap) + 255) & ~size_t(255);
+    const size_t pol_bytes = (polar_scratch_bytes(ctx->queue_cap, ctx->hash_cap) + 255) & ~size_t(255);
+    for (long long c0 = 0; c0 < n; c0 += kChunk) {
+        const int cn = static_cast<int>((n - c0) < kChunk ? (n - c0) : kChunk);
+        FsWork w{};
+        w.items = static_cast<const FsItem*>(ctx->fs_items.ptr) + c0;
+        w.settings = static_cast<const FsSettingsDev*>(ctx->fs_settings.ptr);
+        w.models = static_cast<const CausticModel*>(ctx->fs_models.ptr);
+        w.raw_offset = static_cast<const long long*>(ctx->fs_raw_offset.ptr);
+        w.raw = static_cast<const P2*>(ctx->fs_raw.ptr);
+        w.branches = static_cast<const P2*>(ctx->fs_branches.ptr);
+        w.ld_tables = static_cast<const double*>(ctx->fs_ld.ptr);
+        w.trig = trig_of(ctx);
+        w.out = static_cast<FsOut*>(ctx->fs_out.ptr) + c0;
+        w.n_items = cn;
+        int* counters = static_cast<int*>(ctx->fs_counters.ptr);
+        w.ir_count = counters;
+        w.next_item = counters + 8;
+        w.ir_cart = static_cast<int*>(ctx->fs_ir.ptr);
+        w.ir_polar = w.ir_cart + kChunk;
+        w.seeds = static_cast<P2*>(ctx->fs_seeds.ptr);
+        w.seed_cap = ctx->seed_cap;
+        w.scratch = static_cast<char*>(ctx->fs_scratch.ptr);
+        w.scratch_per_warp = static_cast<long long>(cart_bytes);
+        w.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar.ptr);
+        w.scratch_polar_per_warp = static_cast<long long>(pol_bytes);
+        w.row_cap = ctx->row_cap;
+        w.queue_cap = ctx->queue_cap;
+        w.hash_cap = ctx->hash_cap;
+        w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr) + c0;
+        w.retry_pass = 0;
+        w.retry_cart = static_cast<int*>(ctx->fs_retry.ptr);
+        w.retry_polar = w.retry_cart + kChunk;
+        if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
+        cudaEvent_t ev;
+        ctx->stage_begin(1, &ev);
+        if (!ctx->check("decide", launch_decide(w, ctx->sm_count, ctx->stream))) return false;
+        ctx->stage_end(1, ev);
+        const int warps = ctx->fs_warps < cn ? ctx->fs_warps : cn;
+        // Candidate keys and probes share one allocation: all warps' keys, then all probes.
+        const size_t per = seed_candidate_bytes_per_warp();
+        const size_t key_bytes = per * 8 / (8 + 16);
+        char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
+        ctx->stage_begin(2, &ev);
+        if (!ctx->check("seeds", launch_seeds(w, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
+                                              reinterpret_cast<P2*>(cb + key_bytes * ctx->fs_warps), warps)))
+            return false;
+        ctx->stage_end(2, ev);
+        if (++ctx->epoch >= 0xfff0ull) {
+            ctx->big_ready = false;
+            if (!ensure_big_scratch(ctx)) return false;
+            if (!ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart_bytes * ctx->fs_warps,
+                                                             ctx->stream)) ||
+                !ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff,
+                                                             pol_bytes * ctx->fs_warps, ctx->stream)))
+                return false;
+            ctx->epoch = 1;
+        }
+        ctx->stage_begin(3, &ev);
+        if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
+        ctx->stage_end(3, ev);
+        ctx->stage_begin(4, &ev);
+        if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) return false;
+        ctx->stage_end(4, ev);
+        // Second pass over the items that outgrew the first pass's scratch.
+        FsWork r = w;
+        r.retry_pass = 1;
+        r.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
+        r.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
+        r.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar_big.ptr);
+        r.scratch_polar_per_warp = static_cast<long long>(polar_bytes_big(ctx));
+        r.row_cap = ctx->row_cap_big;
+        r.queue_cap = ctx->queue_cap_big;
+        r.hash_cap = ctx->hash_cap_big;
+        ctx->stage_begin(3, &ev);
+        if (!ctx->check("cartesian retry", launch_cartesian(r, ctx->retry_warps, ctx->stream, ctx->epoch))) return false;
+        ctx->stage_end(3, ev);
+        ctx->stage_begin(4, &ev);
+        if (!ctx->check("polar retry", launch_polar(r, ctx->retry_warps, ctx->stream, ctx->epoch))) return false;
+        ctx->stage_end(4, ev);
+        ctx->launches += 2;
+        ctx->launches += 4;
+    }
+    return true;
+}
+
+int finish_results(Context* ctx, lcbi_fs_result* results, long long n)
+{
+    if (!ctx->check("results D2H", cudaMemcpyAsync(results, ctx->fs_out.ptr, n * sizeof(lcbi_fs_result),
+                                                   cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+bool check_settings(Context* ctx, const lcbi_fs_settings* s, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        if (s[i].adaptive_source_bins != 0 && (s[i].finite_source_tol > 0.0 || s[i].finite_source_reltol > 0.0))
+            return ctx->fail("adaptive source bins (local refinement) is not implemented");
+        if (s[i].finite_mode == 3) return ctx->fail("finite_mode 3 (experimental spine integrator) is not implemented");
+    }
+    return true;
+}
+
+} // namespace
+} // namespace lcbi
+
+using namespace lcbi;
+
+extern "C" {
+
+int lcbi_gpu_binary_mag(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_settings,
+                        const lcbi_lens_model* models, int32_t n_models, int64_t n, const lcbi_fs_point* points,
+                        lcbi_fs_result* results, unsigned flags)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0 || !settings || n_settings <= 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!points || !results) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    if (!check_settings(ctx, settings, n_settings)) return LCBI_UNSUPPORTED;
+    const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
+    const bool given = (flags & LCBI_GPU_MODELS_GIVEN) != 0;
+    if (dev && !given) return LCBI_INVALID_ARGUMENT;
+    Plan plan;
+    add_settings(plan, settings, n_settings);
+    ModelTable mt{&plan};
+    std::vector<FsItem> items;
+    if (given) {
+        for (int m = 0; m < n_models; ++m) mt.get(models[m].s, models[m].q, models[m].caustic_bins);
+    }
+    if (!dev) {
+        items.resize(static_cast<size_t>(n));
+        std::memcpy(items.data(), points, n * sizeof(FsItem));
+        for (auto& it : items) {
+            if (it.settings < 0 || it.settings >= n_settings) return LCBI_INVALID_ARGUMENT;
+            if (given) {
+                if (it.model < 0 || it.model >= n_models) return LCBI_INVALID_ARGUMENT;
+            } else if (it.rho > 0.0 && settings[it.settings].finite_mode > 0) {
+                it.model = mt.get(it.s, it.q, settings[it.settings].caustic_bins);
+            } else {
+                it.model = 0;
+            }
+        }
+        if (!upload(ctx, ctx->fs_items, items)) return LCBI_GPU_ERROR;
+    } else {
+        if (!ctx->ensure(ctx->fs_items, n * sizeof(FsItem)) ||
+            !ctx->check("items D2D", cudaMemcpyAsync(ctx->fs_items.ptr, points, n * sizeof(FsItem),
+                                                     cudaMemcpyDeviceToDevice, ctx->stream)))
+            return LCBI_GPU_ERROR;
+    }
+    if (!ctx->ensure(ctx->fs_out, n * sizeof(FsOut))) return LCBI_GPU_ERROR;
+    if (!run_pipeline(ctx, plan, n)) return LCBI_GPU_ERROR;
+    if (dev) {
+        if (!ctx->check("results D2D", cudaMemcpyAsync(results, ctx->fs_out.ptr, n * sizeof(FsOut),
+                                                       cudaMemcpyDeviceToDevice, ctx->stream)) ||
+            !ctx->finish())
+            return LCBI_GPU_ERROR;
+        return LCBI_OK;
+    }
+    return finish_results(ctx, results, n);
+}
+
+int lcbi_gpu_binary_inverse_ray(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int64_t n, const double* s,
+                                const double* q, const double* y1, const double* y2, const double* rho, double* A,
+                                int32_t* method, int32_t* status)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !settings || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!s || !q || !y1 || !y2 || !rho || !A) return LCBI_INVALID_ARGUMENT;
+    lcbi_fs_settings st = *settings;
+    st.kinji_threshold = 1e18;
+    st.hex_threshold = 0.0;
+    st.adaptive_hex_threshold = 0.0;
+    std::vector<lcbi_fs_point> pts(static_cast<size_t>(n));
+    for (long long i = 0; i < n; ++i) {
+        lcbi_fs_point& p = pts[i];
+        p.s = s[i];
+        p.q = q[i];
+        p.y1 = y1[i];
+        p.y2 = y2[i];
+        p.rho = std::fabs(rho[i]);
+        p.point_source_magnification = 0.0;
+        p.settings = 0;
+        p.model = 0;
+        p.flags = LCBI_FS_PS_EXACT | LCBI_FS_PS_ON_DEVICE;
+        p.reserved = 0;
+    }
+    std::vector<lcbi_fs_result> res(static_cast<size_t>(n));
+    const int rc = lcbi_gpu_binary_mag(c, &st, 1, nullptr, 0, n, pts.data(), res.data(), 0);
+    if (rc != LCBI_OK) return rc;
+    for (long long i = 0; i < n; ++i) {
+        A[i] = res[i].magnification;
+        if (method) method[i] = res[i].method;
+        if (status) status[i] = res[i].status;
+    }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_light_curves(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_models,
+                          const double* params, const int64_t* first, const int32_t* count, const double* times,
+                          int64_t n_times, double* A, int32_t* method, int32_t* status)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !settings || n_models < 0 || n_times < 0) return LCBI_INVALID_ARGUMENT;
+    if (n_models == 0 || n_times == 0) return LCBI_OK;
+    if (!params || !first || !count || !times || !A) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    if (!check_settings(ctx, settings, 1)) return LCBI_UNSUPPORTED;
+    Plan plan;
+    add_settings(plan, settings, 1);
+    ModelTable mt{&plan};
+    std::vector<LcModel> lcm(static_cast<size_t>(n_models));
+    for (int m = 0; m < n_models; ++m) {
+        const double* p = params + 7 * m;
+        if (first[m] < 0 || count[m] < 0 || first[m] + count[m] > n_times) return LCBI_INVALID_ARGUMENT;
+        LcModel& L = lcm[m];
+        L.t0 = p[0];
+        L.tE = p[1];
+        L.u0 = p[2];
+        L.cos_alpha = std::cos(p[3]);
+        L.sin_alpha = std::sin(p[3]);
+        L.s = p[4];
+        L.q_core = p[5] != 0.0 ? 1.0 / p[5] : p[5];
+        L.rho = p[6];
+        L.first = first[m];
+        L.count = count[m];
+        L.settings = 0;
+        L.model = (p[6] != 0.0 && settings->finite_mode > 0) ? mt.get(L.s, L.q_core, settings->caustic_bins) : 0;
+        L.pad = 0;
+    }
+    if (!upload(ctx, ctx->fs_lc_models, lcm) || !ctx->ensure(ctx->fs_times, n_times * sizeof(double)) ||
+        !ctx->check("times H2D", cudaMemcpyAsync(ctx->fs_times.ptr, times, n_times * sizeof(double),
+                                                 cudaMemcpyHostToDevice, ctx->stream)) ||
+        !ctx->ensure(ctx->fs_items, n_times * sizeof(FsItem)) || !ctx->ensure(ctx->fs_out, n_times * sizeof(FsOut)))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("lc items", launch_lc_items(static_cast<LcModel*>(ctx->fs_lc_models.ptr), n_models,
+                                                static_cast<double*>(ctx->fs_times.ptr),
+                                                static_cast<FsItem*>(ctx->fs_items.ptr), n_times, ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    if (!run_pipeline(ctx, plan, n_times)) return LCBI_GPU_ERROR;
+    std::vector<lcbi_fs_result> res(static_cast<size_t>(n_times));
+    const int rc = finish_results(ctx, res.data(), n_times);
+    if (rc != LCBI_OK) return rc;
+    for (long long i = 0; i < n_times; ++i) {
+        A[i] = res[i].magnification;
+        if (method) method[i] = res[i].method;
+        if (status) status[i] = res[i].status;
+    }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_last_ray_counts(lcbi_gpu_context* c, int64_t n, uint64_t* rays)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !rays || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (ctx->fs_rays.ptr == nullptr || (size_t)n * sizeof(uint64_t) > ctx->fs_rays.bytes) return LCBI_INVALID_ARGUMENT;
+    if (!ctx->check("rays D2H", cudaMemcpyAsync(rays, ctx->fs_rays.ptr, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                                ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+} // extern "C"

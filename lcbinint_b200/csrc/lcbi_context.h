@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace lcbi {
@@ -27,12 +28,48 @@ struct Context {
     Buffer out[8];
     Buffer work[8];
 
+    // finite-source pipeline
+    Buffer fs_settings, fs_models, fs_raw_offset, fs_phases, fs_items, fs_out, fs_raw, fs_branches, fs_ld;
+    Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
+    Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
+    bool trig_ready = false;
+    unsigned long long epoch = 0;
+    int fs_warps = 0;          // persistent warps the scratch areas are sized for
+    int row_cap = 32768;       // Cartesian rows per seed scan
+    int queue_cap = 1 << 16;   // polar FIFO of segments
+    int hash_cap = 1 << 17;    // polar visited-segment slots
+    int seed_cap = 2048;       // seeds per inverse-ray item
+    int warps_per_sm = 8;
+    // Second pass for the items that overflow the per-warp scratch above.
+    int retry_warps = 32;
+    int row_cap_big = 1 << 20;
+    int queue_cap_big = 1 << 20;
+    int hash_cap_big = 1 << 21;
+    bool big_ready = false;
+    cudaStream_t own_stream = nullptr;  // the context's stream; `stream` may be a caller's
+
+    // Optional per-stage kernel timing with CUDA events on the launch stream.
+    static constexpr int kStages = 8;  // 0 caustics+LD, 1 decide, 2 seeds, 3 cartesian, 4 polar, 5 point source
+    bool timing = false;
+    double stage_ms[kStages] = {};
+    long long stage_launches[kStages] = {};
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    void stage_begin(int stage, cudaEvent_t* ev);
+    void stage_end(int stage, cudaEvent_t begin);
+    void collect_timing();
+
     std::vector<Buffer*> all_buffers()
     {
         std::vector<Buffer*> v;
         for (auto& b : in) v.push_back(&b);
         for (auto& b : out) v.push_back(&b);
         for (auto& b : work) v.push_back(&b);
+        for (Buffer* b : {&fs_settings, &fs_models, &fs_raw_offset, &fs_phases, &fs_items, &fs_out, &fs_raw,
+                          &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
+                          &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
+                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big})
+            v.push_back(b);
         return v;
     }
 

@@ -1,0 +1,105 @@
+// Internal launch interface of the finite-source kernels (not public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lcbi_fs.cuh"
+
+namespace lcbi {
+
+// One finite-source evaluation: FiniteSourceMagnifier::binary_mag arguments
+// (finite_source_magnifier.cpp:4633-4642) plus table indices.
+struct FsItem {
+    double s, q, x, y, rho, a_ps;
+    int settings;   // index into the FsSettingsDev table
+    int model;      // index into the CausticModel table
+    int flags;      // kItemPsExact | kItemPsOnDevice
+    int pad;
+};
+
+enum : int {
+    kItemPsExact = 1,     // point_source_magnification_is_exact (hexadecapole reuses a_ps)
+    kItemPsOnDevice = 2,  // a_ps = binary_mag0(s, q, x, y), computed by the decision kernel
+};
+
+// Per-item outputs.
+struct FsOut {
+    double A;
+    double err;
+    int method;     // FiniteSourceMethod value
+    int converged;
+    int status;     // 0 ok, 2 numerical error, 16+ device-side limit hit
+    int n_seeds;
+};
+
+// Device-side limits; exceeding one sets FsOut::status and the item's A to NaN.
+enum FsStatus {
+    kFsOk = 0,
+    kFsNumerical = 2,
+    kFsSeedOverflow = 17,
+    kFsRowOverflow = 18,
+    kFsQueueOverflow = 19,
+    kFsHashOverflow = 20,
+};
+
+struct FsWork {
+    const FsItem* items;
+    const FsSettingsDev* settings;
+    const CausticModel* models;
+    const long long* raw_offset;
+    const P2* raw;
+    const P2* branches;
+    const double* ld_tables;
+    TrigTables trig;
+    FsOut* out;
+    int n_items;
+    // inverse-ray work lists written by the decision kernel
+    int* ir_count;   // [0] cartesian, [1] polar
+    int* ir_cart;
+    int* ir_polar;
+    // seeds
+    P2* seeds;       // seed_cap per inverse-ray item, indexed by item
+    int seed_cap;
+    // per-warp scratch for the Cartesian row scan and the polar flood fill
+    char* scratch;
+    long long scratch_per_warp;
+    char* scratch_polar;
+    long long scratch_polar_per_warp;
+    int row_cap;     // Cartesian rows per seed scan
+    int queue_cap;   // polar FIFO of segments (power of two)
+    int hash_cap;    // polar visited-segment hash slots (power of two)
+    int* next_item;  // dynamic work counters: [0] seeds, [1] cartesian, [2] polar, [3] cart retry, [4] polar retry
+    unsigned long long* rays;  // per item: lattice cells whose centre maps inside the source disk
+    // Items whose scratch overflowed in the first pass are queued here and run
+    // again with a larger per-warp scratch (retry_pass = 1); counts in ir_count[2..3].
+    int retry_pass;
+    int* retry_cart;
+    int* retry_polar;
+};
+
+cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables, cudaStream_t stream);
+cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,
+                            const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream);
+cudaError_t launch_decide(const FsWork& w, int sm_count, cudaStream_t stream);
+cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, long long* cand_keys, P2* cand_probes,
+                         int n_warps);
+cudaError_t launch_cartesian(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
+cudaError_t launch_polar(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
+size_t seed_candidate_bytes_per_warp();
+size_t cartesian_scratch_bytes(int row_cap, int seed_cap);
+size_t polar_scratch_bytes(int queue_cap, int hash_cap);
+
+// Source positions of static-binary light curves in VBM convention
+// (python/lcbinint_pybind.cpp:1140-1157): one item per epoch.
+struct LcModel {
+    double t0, tE, u0, cos_alpha, sin_alpha, s, q_core, rho;
+    long long first;  // first epoch index in the times array
+    int count;
+    int settings;
+    int model;        // caustic model index
+    int pad;
+};
+cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* times, FsItem* items,
+                            long long n_items, cudaStream_t stream);
+
+} // namespace lcbi

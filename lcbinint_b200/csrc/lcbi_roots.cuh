@@ -38,7 +38,7 @@ __device__ __forceinline__ double jump(int k)
 }
 
 // Random-direction escape used only when a derivative is exactly zero.
-__device__ __noinline__ dc escape_dir(double angle)
+static __device__ __noinline__ dc escape_dir(double angle)
 {
     double s, c;
     sincos(angle, &s, &c);

@@ -203,6 +203,8 @@ int orc_critical_sources(double s, double q, double phi, double* out)
 
 double orc_ld_brightness(double c, double d, double r2) { return oracle::ld_brightness(c, d, r2); }
 
+int orc_last_max_rows() { return oracle::last_max_rows(); }
+
 // Static-binary light curve in VBM convention (python/lcbinint_pybind.cpp:1087-1174).
 int orc_light_curve_static(const CSettings* cst, const double* times, int n, double t0, double tE, double u0,
                            double alpha, double s, double q, double rho, double* out, int* method)

@@ -678,12 +678,15 @@ void augment_from_branches(const CausticCache& cc, double s, double q, Pt src, d
 
 // ----- Cartesian row scan (FSM:911-930, 1891-2014, 2470-2768) -----
 
+int g_max_rows = 0;  // largest row count of one seed's scans in the last call (diagnostics)
+
 struct Rows {
     std::vector<double> xmin, xmax, ax, y, dys;
     std::unordered_map<int, std::vector<int>> keys;
     void ensure(size_t i)
     {
         if (xmin.size() <= i) {
+            if (static_cast<int>(i + 1) > g_max_rows) g_max_rows = static_cast<int>(i + 1);
             xmin.resize(i + 1);
             xmax.resize(i + 1);
             ax.resize(i + 1);
@@ -1121,9 +1124,12 @@ std::vector<Pt> seeds(const FsSettings& st, double s, double q, double x, double
     return v;
 }
 
+int last_max_rows() { return g_max_rows; }
+
 double cartesian(const FsSettings& st, double s, double q, double x, double y, double rho,
                  const std::vector<Pt>& sd, CartesianDiagnostics* diag)
 {
+    g_max_rows = 0;
     const LdTable ld(st);
     return cartesian_impl(st, ld, s, q, {x, y}, rho, sd, diag);
 }

@@ -94,4 +94,7 @@ int critical_sources(double s, double q, double phi, Pt* out);
 
 double ld_brightness(double c, double d, double r2);
 
+// Largest row count one seed's scans reached in the last cartesian() call.
+int last_max_rows();
+
 } // namespace oracle

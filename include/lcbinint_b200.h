@@ -56,6 +56,10 @@ int lcbi_gpu_set_timing(lcbi_gpu_context *ctx, int enable);
  * enabled: 0 caustics + limb-darkening tables, 1 decision, 2 seeding,
  * 3 Cartesian inverse ray, 4 polar inverse ray, 5 point source. */
 int lcbi_gpu_stage_times(const lcbi_gpu_context *ctx, double *ms, int64_t *launches, int32_t n);
+/* Enables per-point clock64 cycle counts of seeding + inverse-ray integration
+ * (instrumentation, read back with lcbi_gpu_last_item_cycles). */
+int lcbi_gpu_set_item_cycles(lcbi_gpu_context *ctx, int enable);
+int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles);
 /* Device-measured FP64 fused-multiply-add throughput of this GPU in TFLOP/s
  * (2 flop per FMA), the denominator of the FP64 roofline; no reference counterpart. */
 int lcbi_gpu_measure_fp64_peak(lcbi_gpu_context *ctx, double *tflops);

@@ -76,6 +76,10 @@ def _declare(L):
     L.lcbi_gpu_stage_times.restype = C.c_int
     L.lcbi_gpu_measure_fp64_peak.argtypes = [_vp, _vp]
     L.lcbi_gpu_measure_fp64_peak.restype = C.c_int
+    L.lcbi_gpu_set_item_cycles.argtypes = [_vp, C.c_int]
+    L.lcbi_gpu_set_item_cycles.restype = C.c_int
+    L.lcbi_gpu_last_item_cycles.argtypes = [_vp, C.c_int64, _vp]
+    L.lcbi_gpu_last_item_cycles.restype = C.c_int
     L.lcbi_gpu_last_ray_counts.argtypes = [_vp, C.c_int64, _vp]
     L.lcbi_gpu_last_ray_counts.restype = C.c_int
 

@@ -203,6 +203,14 @@ int lcbi_gpu_set_timing(lcbi_gpu_context* c, int enable)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_item_cycles(lcbi_gpu_context* c, int enable)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->item_cycles = enable != 0;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_stage_times(const lcbi_gpu_context* c, double* ms, int64_t* launches, int32_t n)
 {
     const Context* ctx = reinterpret_cast<const Context*>(c);

@@ -72,7 +72,7 @@ bool ensure_scratch(Context* ctx)
     const size_t cart = (cartesian_scratch_bytes(ctx->row_cap, ctx->seed_cap) + 255) & ~size_t(255);
     const size_t pol = (polar_scratch_bytes(ctx->queue_cap, ctx->hash_cap) + 255) & ~size_t(255);
     if (!ctx->ensure(ctx->fs_scratch, cart * warps) || !ctx->ensure(ctx->fs_scratch_polar, pol * warps) ||
-        !ctx->ensure(ctx->fs_cand_keys, seed_candidate_bytes_per_warp() * warps))
+        !ctx->ensure(ctx->fs_cand_keys, seed_candidate_bytes_per_warp(ctx->cand_cap) * warps))
         return false;
     if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart * warps, ctx->stream)) ||
         !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff, pol * warps, ctx->stream)))
@@ -208,6 +208,11 @@ bool upload(Context* ctx, Buffer& b, const std::vector<T>& v)
 // results to ctx->fs_out.  Everything is asynchronous on ctx->stream.
 bool run_pipeline(Context* ctx, const Plan& plan, long long n)
 {
+    // Candidate lists of the caustic-branch seed probes hold one entry per sampled point.
+    if (4 * plan.max_bins > ctx->cand_cap) {
+        ctx->cand_cap = 4 * plan.max_bins;
+        ctx->fs_warps = 0;  // re-size the per-warp areas
+    }
     if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx)) return false;
     const int nset = static_cast<int>(plan.settings.size());
     const int nmod = static_cast<int>(plan.models.size());
@@ -222,6 +227,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         !ctx->ensure(ctx->fs_branches, (raw_total + 1) * sizeof(P2)) ||
         !ctx->ensure(ctx->fs_ld, (size_t)(nld + 1) * (kLdTable + 1) * sizeof(double)) ||
         !ctx->ensure(ctx->fs_rays, (size_t)(n + 1) * sizeof(unsigned long long)) ||
+        (ctx->item_cycles && !ctx->ensure(ctx->fs_cycles, (size_t)(n + 1) * sizeof(long long))) ||
         !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
         !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
         !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)) ||
@@ -236,6 +242,9 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
     ctx->launches += 1;
     if (!ctx->check("rays init", cudaMemsetAsync(ctx->fs_rays.ptr, 0, (size_t)n * sizeof(unsigned long long),
                                                  ctx->stream)))
+        return false;
+    if (ctx->item_cycles &&
+        !ctx->check("cycles init", cudaMemsetAsync(ctx->fs_cycles.ptr, 0, (size_t)n * sizeof(long long), ctx->stream)))
         return false;
     if (nmod > 0) {
         if (!ctx->check("caustics", launch_caustics(static_cast<CausticModel*>(ctx->fs_models.ptr), nmod, plan.max_bins,
@@ -280,6 +289,8 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         w.retry_pass = 0;
         w.retry_cart = static_cast<int*>(ctx->fs_retry.ptr);
         w.retry_polar = w.retry_cart + kChunk;
+        w.cand_cap = ctx->cand_cap;
+        w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
         if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
         cudaEvent_t ev;
         ctx->stage_begin(1, &ev);
@@ -287,7 +298,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         ctx->stage_end(1, ev);
         const int warps = ctx->fs_warps < cn ? ctx->fs_warps : cn;
         // Candidate keys and probes share one allocation: all warps' keys, then all probes.
-        const size_t per = seed_candidate_bytes_per_warp();
+        const size_t per = seed_candidate_bytes_per_warp(ctx->cand_cap);
         const size_t key_bytes = per * 8 / (8 + 16);
         char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
         ctx->stage_begin(2, &ev);
@@ -501,6 +512,20 @@ int lcbi_gpu_light_curves(lcbi_gpu_context* c, const lcbi_fs_settings* settings,
         if (method) method[i] = res[i].method;
         if (status) status[i] = res[i].status;
     }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_last_item_cycles(lcbi_gpu_context* c, int64_t n, int64_t* cycles)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !cycles || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!ctx->item_cycles || ctx->fs_cycles.ptr == nullptr || (size_t)n * sizeof(int64_t) > ctx->fs_cycles.bytes)
+        return LCBI_INVALID_ARGUMENT;
+    if (!ctx->check("cycles D2H", cudaMemcpyAsync(cycles, ctx->fs_cycles.ptr, n * sizeof(int64_t),
+                                                  cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
     return LCBI_OK;
 }
 

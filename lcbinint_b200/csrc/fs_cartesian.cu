@@ -371,6 +371,7 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
         if (k >= n) break;
         if (w.retry_pass) k = w.retry_cart[k];
         const int it = w.ir_cart[k];
+        const long long t_item = clock64();
         const FsItem item = w.items[it];
         FsOut o = w.out[it];
         if (o.status != kFsOk) continue;
@@ -540,7 +541,10 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
         o.A = A;
         if (ovf) o.status = kFsRowOverflow;
         else if (!isfinite(A)) o.status = kFsNumerical;
-        if (lane == 0) w.out[it] = o;
+        if (lane == 0) {
+            w.out[it] = o;
+            if (w.cycles) w.cycles[it] += clock64() - t_item;
+        }
         __syncwarp();
     }
 }

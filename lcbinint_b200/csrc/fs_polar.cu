@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(128) polar_kernel(FsWork w, unsigned long long
         if (k >= n) break;
         if (w.retry_pass) k = w.retry_polar[k];
         const int it = w.ir_polar[k];
+        const long long t_item = clock64();
         const FsItem item = w.items[it];
         FsOut o = w.out[it];
         if (o.status != kFsOk) continue;
@@ -338,7 +339,10 @@ __global__ void __launch_bounds__(128) polar_kernel(FsWork w, unsigned long long
         o.converged = isfinite(A) ? 1 : 0;
         if (P.ovf) o.status = kFsQueueOverflow;
         else if (!isfinite(A)) o.status = kFsNumerical;
-        if (lane == 0) w.out[it] = o;
+        if (lane == 0) {
+            w.out[it] = o;
+            if (w.cycles) w.cycles[it] += clock64() - t_item;
+        }
         __syncwarp();
     }
 }

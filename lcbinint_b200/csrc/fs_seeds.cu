@@ -19,7 +19,10 @@ namespace {
 constexpr int kPhaseSamples = 1400;  // FSM:1741
 constexpr int kSkip = 40;            // FSM:1745
 constexpr int kMaxBoundarySeeds = 128;
-constexpr int kCandCap = 512;        // caustic-branch probe candidates per item
+
+
+// Caustic-branch probe candidates per warp: at most one per sampled caustic
+// point, so 4 x caustic_bins (FsWork::cand_cap) always suffices.
 
 struct WarpShared {
     P2 img[32][5];
@@ -230,7 +233,7 @@ __device__ void ring_probes(SeedState& S, double pr, const double2* table, int c
 
 // augment_seeds_from_caustic_branches (FSM:4845-4926).
 __device__ void augment_from_branches(SeedState& S, const CausticModel& md, const P2* __restrict__ br,
-                                      long long* cand_key, P2* cand_probe)
+                                      long long* cand_key, P2* cand_probe, int kCandCap)
 {
     if (S.n >= 5) return;
     const double R = S.rho + md.max_seg_len;
@@ -314,8 +317,8 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
     extern __shared__ __align__(16) unsigned char smem[];
     WarpShared* sh = reinterpret_cast<WarpShared*>(smem) + warp_in_block();
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    long long* ck = cand_keys + (long long)gw * 2 * kCandCap;
-    P2* cp = cand_probes + (long long)gw * 2 * kCandCap;
+    long long* ck = cand_keys + (long long)gw * 2 * w.cand_cap;
+    P2* cp = cand_probes + (long long)gw * 2 * w.cand_cap;
     const int n_cart = w.ir_count[0];
     const int total = n_cart + w.ir_count[1];
     for (;;) {
@@ -324,6 +327,7 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
         k = shfl_i(k, 0);
         if (k >= total) break;
         const int it = (k < n_cart) ? w.ir_cart[k] : w.ir_polar[k - n_cart];
+        const long long t_item = clock64();
         const FsItem item = w.items[it];
         const CausticModel md = w.models[item.model];
         SeedState S;
@@ -403,11 +407,12 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
                 for (int r = 0; r < 3; ++r) ring_probes(S, S.rho * fr[r], w.trig.interior, 64, 0);
             }
         }
-        augment_from_branches(S, md, w.branches + md.branch_offset, ck, cp);
+        augment_from_branches(S, md, w.branches + md.branch_offset, ck, cp, w.cand_cap);
         if (lane_id() == 0) {
             FsOut* o = w.out + it;
             o->n_seeds = S.n;
             if (S.ovf) o->status = kFsSeedOverflow;
+            if (w.cycles) w.cycles[it] = clock64() - t_item;
         }
         __syncwarp();
     }
@@ -423,6 +428,6 @@ cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, lon
     return cudaGetLastError();
 }
 
-size_t seed_candidate_bytes_per_warp() { return (size_t)2 * kCandCap * (sizeof(long long) + sizeof(P2)); }
+size_t seed_candidate_bytes_per_warp(int cand_cap) { return (size_t)2 * cand_cap * (sizeof(long long) + sizeof(P2)); }
 
 } // namespace lcbi

@@ -32,6 +32,7 @@ struct Context {
     Buffer fs_settings, fs_models, fs_raw_offset, fs_phases, fs_items, fs_out, fs_raw, fs_branches, fs_ld;
     Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
     Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
+    Buffer fs_cycles;
     bool trig_ready = false;
     unsigned long long epoch = 0;
     int fs_warps = 0;          // persistent warps the scratch areas are sized for
@@ -39,6 +40,8 @@ struct Context {
     int queue_cap = 1 << 16;   // polar FIFO of segments
     int hash_cap = 1 << 17;    // polar visited-segment slots
     int seed_cap = 2048;       // seeds per inverse-ray item
+    int cand_cap = 4 * 1400;   // caustic-branch probe candidates per warp
+    bool item_cycles = false;  // record per-item seeding + integration cycles
     int warps_per_sm = 8;
     // Second pass for the items that overflow the per-warp scratch above.
     int retry_warps = 32;
@@ -68,7 +71,7 @@ struct Context {
         for (Buffer* b : {&fs_settings, &fs_models, &fs_raw_offset, &fs_phases, &fs_items, &fs_out, &fs_raw,
                           &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
                           &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
-                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big})
+                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles})
             v.push_back(b);
         return v;
     }

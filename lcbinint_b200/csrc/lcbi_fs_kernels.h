@@ -75,6 +75,8 @@ struct FsWork {
     int retry_pass;
     int* retry_cart;
     int* retry_polar;
+    int cand_cap;                  // caustic-branch probe candidates per warp (4 x max caustic bins)
+    long long* cycles;             // optional per-item clock64 cycles of seeding + integration
 };
 
 cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables, cudaStream_t stream);
@@ -85,7 +87,7 @@ cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, lon
                          int n_warps);
 cudaError_t launch_cartesian(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
 cudaError_t launch_polar(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
-size_t seed_candidate_bytes_per_warp();
+size_t seed_candidate_bytes_per_warp(int cand_cap);
 size_t cartesian_scratch_bytes(int row_cap, int seed_cap);
 size_t polar_scratch_bytes(int queue_cap, int hash_cap);
 

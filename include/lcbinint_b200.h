@@ -183,6 +183,39 @@ int lcbi_gpu_light_curves(lcbi_gpu_context *ctx, const lcbi_fs_settings *setting
  * accounting; no reference counterpart.  n must not exceed that call's size. */
 int lcbi_gpu_last_ray_counts(lcbi_gpu_context *ctx, int64_t n, uint64_t *rays);
 
+/* Finite-source magnification that allocates nothing.  No reference
+ * counterpart: the reference allocates freely on the host, and the entry
+ * points above grow per-context device workspaces (cudaMalloc, and cudaFree of
+ * the smaller buffer, which waits for the whole device) whenever a batch
+ * outgrows them.  Callers that cannot allow that -- a sampler that has reserved
+ * all free device memory for its own pool, or one whose other streams must not
+ * be stalled by a device-wide wait -- use this entry point instead.
+ *
+ * It runs the pipeline of lcbi_gpu_binary_mag for one lens model (s, q) and one
+ * settings struct, with the point-source magnification computed on the device
+ * (LCBI_FS_PS_ON_DEVICE | LCBI_FS_PS_EXACT), and gives the same results as
+ * lcbi_gpu_binary_mag on those points.  y1, y2, rho and results are DEVICE
+ * arrays of n entries; settings is a host pointer.  All working memory is one
+ * fixed device array of LCBI_NOALLOC_AREA_BYTES (48 MiB) per device, reserved
+ * when the library's device code is loaded on that device:
+ *   - settings->caustic_bins above LCBI_NOALLOC_MAX_CAUSTIC_BINS is rejected
+ *     with LCBI_INVALID_ARGUMENT and a message in lcbi_gpu_last_error;
+ *   - a point whose Cartesian scan needs more than 65536 rows, or whose polar
+ *     flood fill holds more than 131072 segments, gets status 18 / 19 (the
+ *     workspace entry points go on to 1048576).
+ * The first call on a device does a one-time setup (it looks up the fixed
+ * array's device address, which loads the library's device code on that device,
+ * and uploads constant angle tables); make that first call -- n = 0 is enough --
+ * before any stream capture begins.  Calls on one device share the one array:
+ * calls that overlap in time (two host threads, or two streams without
+ * ordering between them) race on it, so serialise them.  The call returns after
+ * its work on the context's stream has finished. */
+#define LCBI_NOALLOC_MAX_CAUSTIC_BINS 2048
+#define LCBI_NOALLOC_AREA_BYTES (48u << 20)
+int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, double s, double q,
+                                int64_t n, const double *y1, const double *y2, const double *rho,
+                                lcbi_fs_result *results);
+
 #ifdef __cplusplus
 }
 #endif

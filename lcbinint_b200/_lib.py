@@ -82,6 +82,8 @@ def _declare(L):
     L.lcbi_gpu_last_item_cycles.restype = C.c_int
     L.lcbi_gpu_last_ray_counts.argtypes = [_vp, C.c_int64, _vp]
     L.lcbi_gpu_last_ray_counts.restype = C.c_int
+    L.lcbi_gpu_binary_mag_noalloc.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_int64, _vp, _vp, _vp, _vp]
+    L.lcbi_gpu_binary_mag_noalloc.restype = C.c_int
 
 
 def exported_symbols() -> list[str]:

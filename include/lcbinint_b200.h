@@ -60,6 +60,13 @@ int lcbi_gpu_stage_times(const lcbi_gpu_context *ctx, double *ms, int64_t *launc
  * (instrumentation, read back with lcbi_gpu_last_item_cycles). */
 int lcbi_gpu_set_item_cycles(lcbi_gpu_context *ctx, int enable);
 int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles);
+/* Load balance of the finite-source scans (no reference counterpart): a point
+ * whose Cartesian or polar scan passes `cells` lattice cells on its one warp
+ * is moved to a second pass that runs it on a whole block with a larger
+ * scratch.  0 disables the move (points then change pass only when they
+ * outgrow the per-warp scratch); the default is 524288.  Results are the same
+ * for every value. */
+int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
 /* Device-measured FP64 fused-multiply-add throughput of this GPU in TFLOP/s
  * (2 flop per FMA), the denominator of the FP64 roofline; no reference counterpart. */
 int lcbi_gpu_measure_fp64_peak(lcbi_gpu_context *ctx, double *tflops);

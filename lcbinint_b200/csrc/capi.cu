@@ -211,6 +211,14 @@ int lcbi_gpu_set_item_cycles(lcbi_gpu_context* c, int enable)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_cell_budget(lcbi_gpu_context* c, int64_t cells)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || cells < 0) return LCBI_INVALID_ARGUMENT;
+    ctx->cell_budget = cells;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_stage_times(const lcbi_gpu_context* c, double* ms, int64_t* launches, int32_t n)
 {
     const Context* ctx = reinterpret_cast<const Context*>(c);

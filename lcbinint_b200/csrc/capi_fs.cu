@@ -85,11 +85,13 @@ bool ensure_scratch(Context* ctx)
 size_t cart_bytes_big(const Context* c) { return (cartesian_scratch_bytes(c->row_cap_big, c->seed_cap) + 255) & ~size_t(255); }
 size_t polar_bytes_big(const Context* c) { return (polar_scratch_bytes(c->queue_cap_big, c->hash_cap_big) + 255) & ~size_t(255); }
 
+int retry_blocks(const Context* c) { return c->retry_blocks > 0 ? c->retry_blocks : c->sm_count; }
+
 bool ensure_big_scratch(Context* ctx)
 {
     if (ctx->big_ready) return true;
-    const size_t cb = cart_bytes_big(ctx) * ctx->retry_warps;
-    const size_t pb = polar_bytes_big(ctx) * ctx->retry_warps;
+    const size_t cb = cart_bytes_big(ctx) * retry_blocks(ctx);
+    const size_t pb = polar_bytes_big(ctx) * retry_blocks(ctx);
     if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb)) return false;
     if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_big.ptr, 0xff, cb, ctx->stream)) ||
         !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar_big.ptr, 0xff, pb, ctx->stream)))
@@ -291,6 +293,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         w.retry_polar = w.retry_cart + kChunk;
         w.cand_cap = ctx->cand_cap;
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
+        w.cell_budget = ctx->cell_budget;
         if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
         cudaEvent_t ev;
         ctx->stage_begin(1, &ev);
@@ -322,7 +325,8 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         ctx->stage_begin(4, &ev);
         if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) return false;
         ctx->stage_end(4, ev);
-        // Second pass over the items that outgrew the first pass's scratch.
+        // Second pass, one block per point, over the points that passed the cell
+        // budget or outgrew the first pass's scratch.
         FsWork r = w;
         r.retry_pass = 1;
         r.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
@@ -333,10 +337,10 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         r.queue_cap = ctx->queue_cap_big;
         r.hash_cap = ctx->hash_cap_big;
         ctx->stage_begin(3, &ev);
-        if (!ctx->check("cartesian retry", launch_cartesian(r, ctx->retry_warps, ctx->stream, ctx->epoch))) return false;
+        if (!ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
         ctx->stage_end(3, ev);
         ctx->stage_begin(4, &ev);
-        if (!ctx->check("polar retry", launch_polar(r, ctx->retry_warps, ctx->stream, ctx->epoch))) return false;
+        if (!ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
         ctx->stage_end(4, ev);
         ctx->launches += 2;
         ctx->launches += 4;

@@ -15,10 +15,10 @@
 // Limits of the fixed area (LCBI_NOALLOC_* in the public header): caustic_bins
 // at most 2048 (larger requests are rejected); 2048 image seeds per point
 // (status 17 beyond, as in lcbi_gpu_binary_mag); 8192 rows per Cartesian seed
-// scan and 16384 polar segments in flight in the first pass, with a second
-// pass of four scans at 65536 rows / 131072 segments for the points that
-// overflow (status 18 / 19 beyond that, where lcbi_gpu_binary_mag goes on to
-// 1048576).  Points are processed 256 at a time, so n itself is unbounded.
+// scan and 16384 polar segments in flight in the first pass (one warp per
+// point), with a second pass on four blocks (one point per block) at 65536
+// rows / 131072 segments for the points that overflow (status 18 / 19 beyond
+// that, where lcbi_gpu_binary_mag goes on further).  Points are processed 256 at a time, so n itself is unbounded.
 //
 // What must start at zero: the work-list counters (reset with a memset at the
 // start of every 256-point chunk).  The row and segment tables of the scans must
@@ -49,13 +49,13 @@ constexpr int kWarps = 32;            // persistent warps of the first pass
 constexpr int kRows = 8192;           // Cartesian rows per seed scan, first pass
 constexpr int kQueue = 1 << 14;       // polar segments in flight, first pass
 constexpr int kHash = 1 << 15;        // polar visited-segment slots, first pass
-constexpr int kRetryWarps = 4;
+constexpr int kRetryBlocks = 4;       // second pass: blocks of kBigWarps warps
 constexpr int kRowsRetry = 1 << 16;
 constexpr int kQueueRetry = 1 << 17;
 constexpr int kHashRetry = 1 << 18;
-// The scan kernels run 4 warps per block and give every launched warp its own
-// share of the scratch, so both warp counts must be multiples of 4.
-static_assert(kWarps % 4 == 0 && kRetryWarps % 4 == 0, "whole blocks only");
+// The first-pass scan kernels run 4 warps per block and give every launched
+// warp its own share of the scratch, so the warp count must be a multiple of 4.
+static_assert(kWarps % 4 == 0, "whole blocks only");
 constexpr int kTrig = 1400 + 400 + 64 + 16;
 constexpr double kHostPi = 3.14159265358979323846;
 constexpr int kMaxDevices = 64;
@@ -110,7 +110,7 @@ bool scratch_fits(size_t* main_cart, size_t* main_polar, size_t* retry_cart, siz
     *retry_cart = up256(cartesian_scratch_bytes(kRowsRetry, kSeedCap));
     *retry_polar = up256(polar_scratch_bytes(kQueueRetry, kHashRetry));
     const size_t first = kWarps * max3(*main_cart, *main_polar, kCandPerWarp);
-    const size_t second = kRetryWarps * (*retry_cart > *retry_polar ? *retry_cart : *retry_polar);
+    const size_t second = kRetryBlocks * (*retry_cart > *retry_polar ? *retry_cart : *retry_polar);
     return first <= kScratchBytes && second <= kScratchBytes;
 }
 
@@ -332,7 +332,7 @@ extern "C" int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context* c, const lcbi_fs_se
         // first-pass scan outgrew its share; the same bytes serve every scan, so
         // each starts from freshly reset tables.
         const size_t first = kWarps * (main_cart > main_polar ? main_cart : main_polar);
-        const size_t second = kRetryWarps * (retry_cart > retry_polar ? retry_cart : retry_polar);
+        const size_t second = kRetryBlocks * (retry_cart > retry_polar ? retry_cart : retry_polar);
         if (!ctx->check("table reset", cudaMemsetAsync(scratch, 0xff, first, st)) ||
             !ctx->check("cartesian", launch_cartesian(w, warps, st, 1)) ||
             !ctx->check("table reset", cudaMemsetAsync(scratch, 0xff, first, st)) ||
@@ -346,9 +346,9 @@ extern "C" int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context* c, const lcbi_fs_se
         r.queue_cap = kQueueRetry;
         r.hash_cap = kHashRetry;
         if (!ctx->check("table reset", cudaMemsetAsync(scratch, 0xff, second, st)) ||
-            !ctx->check("cartesian retry", launch_cartesian(r, kRetryWarps, st, 1)) ||
+            !ctx->check("cartesian retry", launch_cartesian(r, kRetryBlocks, st, 1)) ||
             !ctx->check("table reset", cudaMemsetAsync(scratch, 0xff, second, st)) ||
-            !ctx->check("polar retry", launch_polar(r, kRetryWarps, st, 1)))
+            !ctx->check("polar retry", launch_polar(r, kRetryBlocks, st, 1)))
             return LCBI_GPU_ERROR;
         ctx->launches += 7;
     }

@@ -1,25 +1,47 @@
-// Cartesian inverse-ray integration, one warp per evaluation
-// (inverse_ray_cartesian_binary_mag, finite_source_magnifier.cpp:2470-2768,
-// with the row-scan flood fill cartesian_image_area_impl, :1891-2014).
+// Cartesian inverse-ray integration (inverse_ray_cartesian_binary_mag,
+// finite_source_magnifier.cpp:2470-2768, with the row-scan flood fill
+// cartesian_image_area_impl, :1891-2014).
 //
 // The reference walks the image plane one cell at a time: each row runs right
 // from the previous row's right edge, then left, with gap repairs and overlap
-// bookkeeping that depend on the order of visits.  A warp reproduces that walk
-// exactly: the lens map of the next 32 cells along the current scan direction
-// is evaluated in parallel (lane l takes the cell l steps ahead, its abscissa
-// built by the same l successive additions the reference performs), and the
-// state machine consumes those results in order.  Row bookkeeping lives in a
-// per-warp global scratch area with the reference's zero-on-growth semantics,
-// and the same-row overlap test uses a direct-mapped table keyed by the
-// reference's integer row key, so the magnification is bit-identical.
+// bookkeeping that depend on the order of visits.  A group of W warps (one
+// warp for ordinary points; a block of kBigWarps warps in the second pass, for
+// points whose scan passed the first pass's cell budget or scratch) reproduces
+// that walk exactly:
+//   * the lens map of the next 32 W cells along the current scan direction is
+//     evaluated in parallel.  The reference reaches the cell t steps ahead by t
+//     successive additions x += dx; inside one binade every such rounded sum
+//     adds the same step, so the abscissa is formed in closed form, one binade
+//     stretch at a time (constant_run), with the single additions that cross
+//     binade boundaries done as the reference does them;
+//   * the scan state machine consumes those results in order: runs of cells
+//     that only accumulate, or only step on, are consumed from ballot masks in
+//     one go; every other cell goes through the reference's loop body;
+//   * row bookkeeping lives in per-group global scratch with the reference's
+//     zero-on-growth vector semantics, and the same-row overlap test uses a
+//     generation-tagged hash of the reference's integer row keys.
+// The brightness sum keeps the reference's summation order, so the
+// magnification is bit-identical.
 #include "lcbi_fs_kernels.h"
-#include "lcbi_warp.cuh"
+#include "lcbi_group.cuh"
 
 #include <cstdint>
 
 namespace lcbi {
 
 namespace {
+
+template <int W>
+struct CartShared {
+    double d[32 * W];   // dz2 of each chunk cell (rho^2 + 1 on the wrong parity)
+    double b[32 * W];   // brightness of inside cells
+    double x[32 * W];   // abscissa of each chunk cell
+    unsigned in[W];     // inside masks
+    unsigned cont[W];   // left scan: abscissa >= xmin(previous row) - dx
+    double sum;         // broadcast of a sequential brightness sum
+    int item;
+    int red[W];
+};
 
 struct RowScratch {
     double* xmin;
@@ -63,6 +85,7 @@ __device__ __forceinline__ int key_lookup(const RowScratch& R, int key, unsigned
     return -1;
 }
 
+template <int W>
 __device__ __forceinline__ void rows_ensure(RowScratch& R, int i)
 {
     if (i < R.hw) return;
@@ -70,7 +93,7 @@ __device__ __forceinline__ void rows_ensure(RowScratch& R, int i)
         R.ovf = true;
         return;
     }
-    for (int r = R.hw + lane_id(); r <= i; r += 32) {
+    for (int r = R.hw + Grp<W>::rank(); r <= i; r += Grp<W>::N) {
         R.xmin[r] = 0.0;
         R.xmax[r] = 0.0;
         R.ax[r] = 0.0;
@@ -78,17 +101,20 @@ __device__ __forceinline__ void rows_ensure(RowScratch& R, int i)
         R.dys[r] = 0.0;
     }
     R.hw = i + 1;
-    __syncwarp();
+    Grp<W>::sync();
 }
 
-// Row values are written by lane 0; every lane keeps the same control flow.
+// Row values are written by rank 0; every thread keeps the same control flow.
+template <int W>
 __device__ __forceinline__ void wset(double* a, int i, double v)
 {
-    if (lane_id() == 0) a[i] = v;
+    if (Grp<W>::rank() == 0) a[i] = v;
 }
 
 struct Ctx {
-    unsigned long long rays;  // inside cells consumed (identical in every lane)
+    unsigned long long rays;  // inside cells consumed (identical in every thread)
+    long long evals;          // cells evaluated (budget accounting)
+    long long budget;         // 0: none
     bool bulk;                // every inside cell has brightness > 0 (run consumption allowed)
     Mapper m;
     P2 src;
@@ -127,10 +153,124 @@ __host__ __device__ inline long long table_slots(int cap)
 
 __device__ __forceinline__ int row_key(double y, double inv_incr) { return to_int_x86(y * inv_incr + kRowKeyOffset); }
 
-// cartesian_image_area_impl: one directional flood fill from `seed`.
-__device__ double image_area(Ctx& C, RowScratch& R, P2 seed, double dy, int& yi, int jsign)
+// True when n repeated additions x0 + d, (x0 + d) + d, ... each add one and the
+// same rounded step, which is then returned: x0 and x0 + n * step lie in one
+// binade (same sign and exponent, the end strictly above the binade's lower
+// bound) and the first two steps agree.  Inside a binade every sum is a
+// multiple of its ulp u, and fl(x + d) = x + (d rounded to a multiple of u);
+// only a d exactly halfway between multiples can alternate between two
+// rounded steps, and then the steps are constant from the first pair of equal
+// steps on.
+__device__ __forceinline__ bool constant_run(double x0, double d, int n, double* step)
 {
-    const int lane = lane_id();
+    if (x0 == 0.0) return false;
+    const double x1 = x0 + d;
+    const double s1 = x1 - x0;
+    const double x2 = x1 + d;
+    if (x2 - x1 != s1) return false;
+    const double xe = x0 + static_cast<double>(n) * s1;
+    int e0, e1;
+    frexp(x0, &e0);
+    const double me = frexp(xe, &e1);
+    if (e0 != e1 || (x0 < 0.0) != (xe < 0.0) || xe == 0.0 || fabs(me) == 0.5) return false;
+    *step = s1;
+    return true;
+}
+
+// x0 after t reference additions of d: binade stretches in closed form (the
+// longest stretch by bisection), the crossings one addition at a time.
+__device__ __forceinline__ double advance(double x0, double d, int t)
+{
+    double x = x0;
+    int k = t;
+    for (int guard = 0; k > 0 && guard < 64; ++guard) {
+        double s;
+        if (constant_run(x, d, k, &s)) {
+            return x + static_cast<double>(k) * s;
+        }
+        int lo = 0, hi = k;  // constant_run holds for lo steps (trivially for 0), fails for hi
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            double sm;
+            if (constant_run(x, d, mid, &sm)) lo = mid;
+            else hi = mid;
+        }
+        if (lo > 0) {
+            double sl;
+            constant_run(x, d, lo, &sl);
+            x = x + static_cast<double>(lo) * sl;
+            k -= lo;
+        }
+        x = x + d;
+        --k;
+    }
+    for (; k > 0; --k) x = x + d;
+    return x;
+}
+
+// Evaluates the chunk of cells starting at ix along dx into shared memory.
+template <int W>
+__device__ void fill_chunk(Ctx& C, CartShared<W>& S, double ix, double iy, double dx, int jsign, bool want_cont,
+                           double thr)
+{
+    const int t = Grp<W>::rank();
+    Grp<W>::sync();  // every thread is done with the previous chunk
+    const double x = advance(ix, dx, t);
+    double d, b;
+    eval_for_scan(C, x, iy, jsign, &d, &b);
+    S.d[t] = d;
+    S.b[t] = b;
+    S.x[t] = x;
+    const unsigned in = __ballot_sync(kFull, d <= C.rho2);
+    const unsigned co = __ballot_sync(kFull, want_cont && x >= thr);
+    if (lane_id() == 0) {
+        S.in[t >> 5] = in;
+        S.cont[t >> 5] = co;
+    }
+    C.evals += Grp<W>::N;
+    Grp<W>::sync();
+}
+
+// First eventful chunk cell at or after `from`: an outside cell while
+// counting; otherwise an inside cell or one past the continue threshold.
+template <int W>
+__device__ __forceinline__ int first_event(const CartShared<W>& S, int from, bool counting)
+{
+    const int fw = from >> 5;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        if (w < fw) continue;
+        const unsigned lo = (w == fw) ? (kFull << (from & 31)) : kFull;
+        const unsigned ev = counting ? (~S.in[w] & lo) : ((S.in[w] | ~S.cont[w]) & lo);
+        if (ev) return (w << 5) + __ffs(ev) - 1;
+    }
+    return Grp<W>::N;
+}
+
+// Sequential brightness sum of chunk cells [a, b) in order, in every thread.
+template <int W>
+__device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a, int b)
+{
+    if (W == 1) {
+        for (int j = a; j < b; ++j) acc += S.b[j];
+        return acc;
+    }
+    if (threadIdx.x == 0) {
+        double v = acc;
+        for (int j = a; j < b; ++j) v += S.b[j];
+        S.sum = v;
+    }
+    __syncthreads();
+    const double r = S.sum;
+    __syncthreads();
+    return r;
+}
+
+// cartesian_image_area_impl: one directional flood fill from `seed`.
+template <int W>
+__device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, double dy, int& yi, int jsign)
+{
+    constexpr int N = Grp<W>::N;
     double countx = 0.0, countall = 0.0, dz2 = 99999999.9;
     const double incr = fabs(dy);
     const double inv_incr = 1.0 / incr;
@@ -138,107 +278,91 @@ __device__ double image_area(Ctx& C, RowScratch& R, P2 seed, double dy, int& yi,
     double ix = seed.x, iy = seed.y;
     double x0 = seed.x;
     int guard = 0;
-    // Speculative chunk: lane l holds the cell l steps from (cx, cy) along cdx.
+    // Chunk: cells [0, N) from (chunk start, cy) along cdx; cidx is the next one to consume.
     bool have = false;
     int cidx = 0;
     double cdx = 0.0, cy = 0.0;
-    double my_x = 0.0, my_d = 0.0, my_b = 0.0;
     for (;;) {
-        if (!(have && cidx < 32 && cdx == dx && cy == iy)) {
-            double x = ix;
-            for (int t = 0; t < 31; ++t)
-                if (t < lane) x = x + dx;
-            my_x = x;
-            eval_for_scan(C, x, iy, jsign, &my_d, &my_b);
+        if (!(have && cidx < N && cdx == dx && cy == iy)) {
+            if (C.budget > 0 && C.evals > C.budget) {
+                R.ovf = true;  // hand the point to the second pass
+                return countall;
+            }
+            const bool want_cont = dx != incr && yi != 0;
+            const double thr = want_cont ? R.xmin[yi - 1] - dx : 0.0;
+            fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr);
             have = true;
             cidx = 0;
             cdx = dx;
             cy = iy;
         }
-        // Bulk step: consume, in one go, the run of cells whose processing only
-        // accumulates (inside cells once the row has a count, or inside cells of
-        // the right scan) or only steps on (outside cells the left scan walks
-        // over before the row's first inside cell).  The next "eventful" cell
-        // goes through the single-cell step below, which is the reference's
-        // loop body verbatim.  Needs every inside cell to have brightness > 0,
-        // so that "countx == 0" means "no inside cell yet".
-        if (C.bulk && guard + 34 < C.max_steps) {
-            const unsigned rem = kFull << cidx;
-            const unsigned ins = __ballot_sync(kFull, my_d <= C.rho2) & rem;
-            unsigned ev;
-            bool counting;
-            if (dx == incr || countx != 0.0) {
-                ev = rem & ~ins;
-                counting = true;
-            } else if (yi != 0) {
-                const double thr = R.xmin[yi - 1] - dx;
-                const unsigned cont = __ballot_sync(kFull, my_x >= thr) & rem;
-                ev = rem & ~(~ins & cont);
-                counting = false;
-            } else {
-                ev = rem;
-                counting = false;
-            }
-            const int stop = ev ? __ffs(ev) - 1 : 32;
-            const int n = stop - cidx;
-            if (n > 0) {
-                if (counting) {
-                    if (C.uniform) {
-                        countx += static_cast<double>(n);
-                    } else {
-                        for (int j = cidx; j < stop; ++j) countx += shfl_d(my_b, j);
+        // Bulk step: consume the run of cells that only accumulate (inside cells of
+        // the right scan, or of the left scan once the row has a count) or only
+        // step on (outside cells the left scan walks over before the row's first
+        // inside cell, while abscissa >= xmin(previous row) + incr).  Needs every
+        // inside cell to have brightness > 0, so "countx == 0" means "no inside
+        // cell yet".
+        if (C.bulk && guard + N + 2 < C.max_steps) {
+            const bool counting = dx == incr || countx != 0.0;
+            if (counting || yi != 0) {
+                const int stop = first_event<W>(S, cidx, counting);
+                const int n = stop - cidx;
+                if (n > 0) {
+                    if (counting) {
+                        if (C.uniform) countx += static_cast<double>(n);
+                        else countx = chunk_sum<W>(S, countx, cidx, stop);
+                        C.rays += n;
                     }
-                    C.rays += n;
+                    guard += n;
+                    dz2 = S.d[stop - 1];
+                    if (stop == N) {
+                        ix = S.x[N - 1] + dx;
+                        have = false;
+                        continue;
+                    }
+                    ix = S.x[stop];
+                    cidx = stop;
                 }
-                guard += n;
-                dz2 = shfl_d(my_d, stop - 1);
-                const double xl = shfl_d(my_x, stop == 32 ? 31 : stop);
-                if (stop == 32) {
-                    ix = xl + dx;
-                    have = false;
-                    continue;
-                }
-                ix = xl;
-                cidx = stop;
             }
         }
+        // Single-cell step: the reference's loop body (FSM:1919-2011).
         if (!(++guard < C.max_steps)) break;
         const double last = dz2;
-        dz2 = shfl_d(my_d, cidx);
-        const double b = shfl_d(my_b, cidx);
+        dz2 = S.d[cidx];
+        const double b = S.b[cidx];
         ++cidx;
-        rows_ensure(R, yi);
+        rows_ensure<W>(R, yi);
         if (R.ovf) return countall;
         if (dz2 <= C.rho2) {
-            if (dx == -incr && countx == 0.0) wset(R.xmax, yi, ix - dx);
+            if (dx == -incr && countx == 0.0) wset<W>(R.xmax, yi, ix - dx);
             countx += b;
             ++C.rays;
         } else if (dx == incr) {
-            if (last <= C.rho2) wset(R.xmax, yi, ix);
+            if (last <= C.rho2) wset<W>(R.xmax, yi, ix);
             dx = -incr;
             ix = x0;
-            wset(R.xmin, yi, ix + dx);
+            wset<W>(R.xmin, yi, ix + dx);
             have = false;
         } else {
-            if (last <= C.rho2) wset(R.xmin, yi, ix);
-            __syncwarp();
+            if (last <= C.rho2) wset<W>(R.xmin, yi, ix);
+            Grp<W>::sync();
             if (yi != 0 && countx == 0.0) {
-                rows_ensure(R, yi - 1);
+                rows_ensure<W>(R, yi - 1);
                 if (ix >= R.xmin[yi - 1] - dx) {
                     ix += dx;
                     continue;
                 }
             }
             countall += countx;
-            wset(R.ax, yi, countx);
-            wset(R.y, yi, iy);
-            wset(R.dys, yi, dy);
+            wset<W>(R.ax, yi, countx);
+            wset<W>(R.y, yi, iy);
+            wset<W>(R.dys, yi, dy);
             if (countx == 0.0) {
-                wset(R.dys, yi, -dy);
-                __syncwarp();
+                wset<W>(R.dys, yi, -dy);
+                Grp<W>::sync();
                 break;
             }
-            __syncwarp();
+            Grp<W>::sync();
             // Same-row overlap with an earlier row of this seed's scans (FSM:1990-1999).
             const int key = row_key(iy, inv_incr);
             unsigned slot;
@@ -253,15 +377,15 @@ __device__ double image_area(Ctx& C, RowScratch& R, P2 seed, double dy, int& yi,
                 if (xmin_y + incr < R.xmax[e] && xmax_y - incr > R.xmin[e]) return countall - countx;
                 e = R.next[e];
             }
-            if (lane == 0) {
+            if (Grp<W>::rank() == 0) {
                 R.next[yi] = head;
                 R.table[slot] = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
                                                            (unsigned long long)(unsigned)(yi + 1));
             }
             ++yi;
-            rows_ensure(R, yi);
+            rows_ensure<W>(R, yi);
             if (R.ovf) return countall;
-            __syncwarp();
+            Grp<W>::sync();
             dx = incr;
             x0 = R.xmax[yi - 1];
             ix = x0 - dx;
@@ -323,29 +447,36 @@ __device__ double area_error(const Diag& d, double rho, int source_bins, double 
 
 // One gap-repair scan (FSM:2576-2663): pre-set the virtual predecessor row,
 // flood from `es` in direction `dy`, drop the rows again if nothing was found.
-__device__ __forceinline__ void repair(Ctx& C, RowScratch& R, P2 es, double xmin_v, double xmax_v, double dy,
-                                       int& yi, int js, double& areai, double& areabound)
+template <int W>
+__device__ __forceinline__ void repair(Ctx& C, RowScratch& R, CartShared<W>& S, P2 es, double xmin_v, double xmax_v,
+                                       double dy, int& yi, int js, double& areai, double& areabound)
 {
-    rows_ensure(R, yi);
+    rows_ensure<W>(R, yi);
     if (R.ovf) return;
-    wset(R.xmin, yi, xmin_v);
-    wset(R.xmax, yi, xmax_v);
-    wset(R.dys, yi, dy);
-    __syncwarp();
+    wset<W>(R.xmin, yi, xmin_v);
+    wset<W>(R.xmax, yi, xmax_v);
+    wset<W>(R.dys, yi, dy);
+    Grp<W>::sync();
     ++yi;
-    const double area0 = image_area(C, R, es, dy, yi, js);
+    const double area0 = image_area<W>(C, R, S, es, dy, yi, js);
+    Grp<W>::sync();  // rows written by rank 0 just before the scan ended
     areai += area0;
     areabound += area0;
     if (area0 <= 0.0) --yi;
 }
 
-} // namespace
+// The list a kernel instance works through.
+struct CartList {
+    const int* slots;   // inverse-ray Cartesian slot of each entry (null: the identity)
+    const int* count;
+    int* next;          // dynamic work counter
+};
 
-__global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long long epoch)
+template <int W>
+__device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S)
 {
-    const int lane = lane_id();
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    char* base = w.scratch + (long long)gw * w.scratch_per_warp;
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
     const int cap = w.row_cap;
     RowScratch R;
     R.xmin = reinterpret_cast<double*>(base);
@@ -353,8 +484,8 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
     R.ax = R.xmax + cap;
     R.y = R.ax + cap;
     R.dys = R.y + cap;
-    // Layout, every array 8-byte aligned: five row arrays and the per-seed areas
-    // (doubles), the row-key table (u64), then the int arrays.
+    // Layout, every array aligned: five row arrays and the per-seed areas
+    // (doubles), the row-key table (16-byte entries), then the int arrays.
     double* areaimage = R.dys + cap;
     R.table = reinterpret_cast<ulonglong2*>((reinterpret_cast<uintptr_t>(areaimage + w.seed_cap) + 15) &
                                             ~static_cast<uintptr_t>(15));
@@ -363,13 +494,14 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
     int* flags = R.next + cap + 2;  // per seed: bit0 overlapped (skip), bit1 subtracted
     R.cap = cap;
     unsigned long long local_gen = 0;
-    const int n = w.retry_pass ? w.ir_count[2] : w.ir_count[0];
+    const int n = *L.count;
     for (;;) {
-        int k = 0;
-        if (lane == 0) k = atomicAdd(&w.next_item[w.retry_pass ? 3 : 1], 1);
-        k = shfl_i(k, 0);
+        Grp<W>::sync();
+        if (t == 0) S.item = atomicAdd(L.next, 1);
+        Grp<W>::sync();
+        int k = S.item;
         if (k >= n) break;
-        if (w.retry_pass) k = w.retry_cart[k];
+        if (L.slots) k = L.slots[k];
         const int it = w.ir_cart[k];
         const long long t_item = clock64();
         const FsItem item = w.items[it];
@@ -381,9 +513,11 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
         const double rho = item.rho;
         double A = dnan();
         bool ovf = false;
+        Ctx C;
+        C.rays = 0;
+        C.evals = 0;
+        C.budget = (W == 1 && !w.retry_pass) ? w.cell_budget : 0;
         if (ns > 0 && rho > 0.0) {
-            Ctx C;
-            C.rays = 0;
             C.m = make_mapper(item.s, item.q);
             C.src = P2{item.x, item.y};
             C.rho = rho;
@@ -398,11 +532,11 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
             const double incr = rho / nbin;
             const double margin = 0.5 * incr * 1.01;
             Diag d{ns, 0, 0, 0, 0, 0, 0.0};
-            for (int i = lane; i < ns; i += 32) {
+            for (int i = t; i < ns; i += N) {
                 areaimage[i] = 0.0;
                 flags[i] = 0;
             }
-            __syncwarp();
+            Grp<W>::sync();
             double area = 0.0;
             for (int ii = 0; ii < ns && !ovf; ++ii) {
                 if (flags[ii] & 1) continue;
@@ -410,7 +544,7 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                 R.gen = (epoch << 32) | (local_gen & 0xffffffffull);
                 R.hw = 0;
                 R.ovf = false;
-                rows_ensure(R, 1);
+                rows_ensure<W>(R, 1);
                 const P2 seed = seeds[ii];
                 double areai = 0.0;
                 double dy = incr;
@@ -419,12 +553,13 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                 const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
                 ++d.processed;
                 if (js != 0) ++d.fold;
-                wset(R.xmin, 0, seed.x);
-                wset(R.xmax, 0, seed.x);
-                __syncwarp();
-                areai = image_area(C, R, seed, dy, yi, js);
+                wset<W>(R.xmin, 0, seed.x);
+                wset<W>(R.xmax, 0, seed.x);
+                Grp<W>::sync();
+                areai = image_area<W>(C, R, S, seed, dy, yi, js);
+                Grp<W>::sync();
                 dy = -incr;
-                rows_ensure(R, yi);
+                rows_ensure<W>(R, yi);
                 if (R.ovf) {
                     ovf = true;
                     break;
@@ -432,41 +567,43 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                 const P2 lower{R.xmax[0], seed.y + dy};
                 {
                     const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
-                    wset(R.xmin, yi, xm0);
-                    wset(R.xmax, yi, xM0);
-                    wset(R.y, yi, y0);
-                    wset(R.dys, yi, dy);
-                    __syncwarp();
+                    Grp<W>::sync();
+                    wset<W>(R.xmin, yi, xm0);
+                    wset<W>(R.xmax, yi, xM0);
+                    wset<W>(R.y, yi, y0);
+                    wset<W>(R.dys, yi, dy);
+                    Grp<W>::sync();
                 }
                 ++yi;
-                areai += image_area(C, R, lower, dy, yi, js);
+                areai += image_area<W>(C, R, S, lower, dy, yi, js);
+                Grp<W>::sync();
                 int nyi = yi;
                 double areabound = 0.0;
                 for (int row = 0; row < nyi && !R.ovf; ++row) {
-                    rows_ensure(R, row + 1);
+                    rows_ensure<W>(R, row + 1);
                     const double dxmax = R.xmax[row + 1] - R.xmax[row];
                     const double dxmin = R.xmin[row + 1] - R.xmin[row];
                     if (R.ax[row + 1] > 0.0) d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
                     if (R.ax[row + 1] > 0.0) {
                         if (dxmax > 1.1 * incr) {
                             ++d.gap_repairs;
-                            repair(C, R, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1], -R.dys[row], yi,
-                                   js, areai, areabound);
+                            repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1],
+                                      -R.dys[row], yi, js, areai, areabound);
                         }
                         if (dxmin > 1.1 * incr) {
                             ++d.gap_repairs;
-                            repair(C, R, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row], R.xmin[row + 1],
-                                   R.dys[row], yi, js, areai, areabound);
+                            repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row],
+                                      R.xmin[row + 1], R.dys[row], yi, js, areai, areabound);
                         }
                         if (dxmin < -1.1 * incr) {
                             ++d.gap_repairs;
-                            repair(C, R, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row], -R.dys[row],
-                                   yi, js, areai, areabound);
+                            repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row],
+                                      -R.dys[row], yi, js, areai, areabound);
                         }
                         if (dxmax < -1.1 * incr) {
                             ++d.gap_repairs;
-                            repair(C, R, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1], R.xmax[row],
-                                   R.dys[row], yi, js, areai, areabound);
+                            repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1],
+                                      R.xmax[row], R.dys[row], yi, js, areai, areabound);
                         }
                     }
                     if (row == nyi - 1 && areabound > 0.0 && yi > nyi) nyi = yi;
@@ -476,9 +613,20 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                     break;
                 }
                 area += areai;
-                if (lane == 0) areaimage[ii] = areai;
-                for (int row = 0; row < nyi; ++row)
-                    if (R.ax[row] > 0.0) ++d.boundary_rows;
+                if (t == 0) areaimage[ii] = areai;
+                {
+                    int br = 0;
+                    for (int row = t; row < nyi; row += N) br += (R.ax[row] > 0.0) ? 1 : 0;
+                    br = warp_sum_i(br);
+                    if (W > 1) {
+                        if (lane_id() == 0) S.red[warp_in_block()] = br;
+                        __syncthreads();
+                        br = 0;
+                        for (int i = 0; i < W; ++i) br += S.red[i];
+                        __syncthreads();
+                    }
+                    d.boundary_rows += br;
+                }
                 // Overlap bookkeeping against every other seed (FSM:2681-2739).
                 for (int oi = 0; oi < ns; ++oi) {
                     if (oi == ii) continue;
@@ -490,14 +638,14 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                             continue;
                     }
                     bool hit = false;
-                    for (int r0 = 0; r0 < nyi; r0 += 32) {
-                        const int row = r0 + lane;
+                    for (int r0 = 0; r0 < nyi; r0 += N) {
+                        const int row = r0 + t;
                         bool h = false;
                         if (row < nyi && R.ax[row] > 0.0) {
                             h = p.y >= R.y[row] - margin && p.y <= R.y[row] + margin &&
                                 p.x >= R.xmin[row] - margin && p.x <= R.xmax[row] + margin;
                         }
-                        if (__any_sync(kFull, h)) {
+                        if (Grp<W>::any(h)) {
                             hit = true;
                             break;
                         }
@@ -508,18 +656,18 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
                             const int f = flags[oi];
                             if (!(f & 2)) {
                                 area -= areaimage[oi];
-                                __syncwarp();
-                                if (lane == 0) flags[oi] = f | 2;
+                                Grp<W>::sync();
+                                if (t == 0) flags[oi] = f | 2;
                             }
                         } else {
-                            if (lane == 0) flags[oi] = flags[oi] | 1;
+                            if (t == 0) flags[oi] = flags[oi] | 1;
                         }
-                        __syncwarp();
+                        Grp<W>::sync();
                     }
                 }
-                __syncwarp();
+                Grp<W>::sync();
             }
-            if (lane == 0) w.rays[it] = C.rays;
+            if (t == 0) w.rays[it] = C.rays;
             if (!ovf) {
                 const double flux = source_flux(rho, st.ld_c, st.ld_d);
                 const double scale = flux / (rho * rho) * nbin * nbin;
@@ -533,21 +681,37 @@ __global__ void __launch_bounds__(128) cartesian_kernel(FsWork w, unsigned long 
             }
         }
         if (ovf && !w.retry_pass) {
-            // Too many rows for this pass's scratch: run again with the large one.
-            if (lane == 0) w.retry_cart[atomicAdd(&w.ir_count[2], 1)] = k;
-            __syncwarp();
+            // Too large for one warp, or for this pass's scratch: the second pass
+            // runs it again on a whole block with the large scratch.
+            if (t == 0) w.retry_cart[atomicAdd(&w.ir_count[2], 1)] = k;
             continue;
         }
         o.A = A;
         if (ovf) o.status = kFsRowOverflow;
         else if (!isfinite(A)) o.status = kFsNumerical;
-        if (lane == 0) {
+        if (t == 0) {
             w.out[it] = o;
             if (w.cycles) w.cycles[it] += clock64() - t_item;
         }
-        __syncwarp();
     }
 }
+
+__global__ void __launch_bounds__(128) cartesian_warp_kernel(FsWork w, unsigned long long epoch)
+{
+    __shared__ CartShared<1> sh[4];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const CartList L{nullptr, w.ir_count + 0, w.next_item + 1};
+    cartesian_body<1>(w, epoch, L, w.scratch + (long long)gw * w.scratch_per_warp, sh[warp_in_block()]);
+}
+
+__global__ void __launch_bounds__(32 * kBigWarps) cartesian_block_kernel(FsWork w, unsigned long long epoch)
+{
+    __shared__ CartShared<kBigWarps> sh;
+    const CartList L{w.retry_cart, w.ir_count + 2, w.next_item + 3};
+    cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh);
+}
+
+} // namespace
 
 size_t cartesian_scratch_bytes(int row_cap, int seed_cap)
 {
@@ -555,10 +719,16 @@ size_t cartesian_scratch_bytes(int row_cap, int seed_cap)
            ((size_t)row_cap + 2 + seed_cap) * sizeof(int) + 256;
 }
 
-cudaError_t launch_cartesian(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch)
+// First pass: one warp per point (n_groups warps).  Second pass
+// (w.retry_pass): one block of kBigWarps warps per point, n_groups blocks,
+// each with its own scratch.
+cudaError_t launch_cartesian(const FsWork& w, int n_groups, cudaStream_t stream, unsigned long long epoch)
 {
-    const int blocks = (n_warps + 3) / 4;
-    cartesian_kernel<<<blocks, 128, 0, stream>>>(w, epoch);
+    if (w.retry_pass) {
+        cartesian_block_kernel<<<n_groups, 32 * kBigWarps, 0, stream>>>(w, epoch);
+    } else {
+        cartesian_warp_kernel<<<(n_groups + 3) / 4, 128, 0, stream>>>(w, epoch);
+    }
     return cudaGetLastError();
 }
 

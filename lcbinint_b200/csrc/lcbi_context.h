@@ -43,10 +43,12 @@ struct Context {
     int cand_cap = 4 * 1400;   // caustic-branch probe candidates per warp
     bool item_cycles = false;  // record per-item seeding + integration cycles
     int warps_per_sm = 8;
-    // Second pass for the items that overflow the per-warp scratch above.
-    int retry_warps = 32;
-    int row_cap_big = 1 << 20;
-    int queue_cap_big = 1 << 20;
+    // Second pass, one block of kBigWarps warps per point, for the points that
+    // pass the first pass's cell budget or overflow its per-warp scratch.
+    long long cell_budget = 1 << 19;
+    int retry_blocks = 0;      // 0: one per SM
+    int row_cap_big = 1 << 19;
+    int queue_cap_big = 1 << 19;
     int hash_cap_big = 1 << 21;
     bool big_ready = false;
     cudaStream_t own_stream = nullptr;  // the context's stream; `stream` may be a caller's

@@ -70,14 +70,21 @@ struct FsWork {
     int hash_cap;    // polar visited-segment hash slots (power of two)
     int* next_item;  // dynamic work counters: [0] seeds, [1] cartesian, [2] polar, [3] cart retry, [4] polar retry
     unsigned long long* rays;  // per item: lattice cells whose centre maps inside the source disk
-    // Items whose scratch overflowed in the first pass are queued here and run
-    // again with a larger per-warp scratch (retry_pass = 1); counts in ir_count[2..3].
+    // Items whose scratch overflowed, or that passed the cell budget, in the
+    // first pass are queued here and run again on whole blocks with a larger
+    // scratch per block (retry_pass = 1); counts in ir_count[2..3].
     int retry_pass;
     int* retry_cart;
     int* retry_polar;
     int cand_cap;                  // caustic-branch probe candidates per warp (4 x max caustic bins)
     long long* cycles;             // optional per-item clock64 cycles of seeding + integration
+    // First pass only: a point whose scan passes this many cells (0: no limit)
+    // is handed to the second pass, which runs each point on a block of
+    // kBigWarps warps.
+    long long cell_budget;
 };
+
+constexpr int kBigWarps = 8;
 
 cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables, cudaStream_t stream);
 cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,

@@ -67,6 +67,10 @@ int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles)
  * outgrow the per-warp scratch); the default is 524288.  Results are the same
  * for every value. */
 int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
+/* Polar inverse ray in the first pass: 1 (default) the tile-parallel flood
+ * fill spread over the whole GPU, 0 the one-warp-per-point segment flood fill.
+ * Both count the same cells; results are the same.  No reference counterpart. */
+int lcbi_gpu_set_polar_tiles(lcbi_gpu_context *ctx, int enable);
 /* Device-measured FP64 fused-multiply-add throughput of this GPU in TFLOP/s
  * (2 flop per FMA), the denominator of the FP64 roofline; no reference counterpart. */
 int lcbi_gpu_measure_fp64_peak(lcbi_gpu_context *ctx, double *tflops);

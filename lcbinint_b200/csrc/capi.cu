@@ -219,6 +219,14 @@ int lcbi_gpu_set_cell_budget(lcbi_gpu_context* c, int64_t cells)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_polar_tiles(lcbi_gpu_context* c, int enable)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->polar_tiles = enable != 0;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_stage_times(const lcbi_gpu_context* c, double* ms, int64_t* launches, int32_t n)
 {
     const Context* ctx = reinterpret_cast<const Context*>(c);

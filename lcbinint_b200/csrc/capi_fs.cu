@@ -233,8 +233,10 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
         !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
         !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)) ||
-        !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)))
+        !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, kChunk)))
         return false;
+    if (ctx->tile_blocks == 0) ctx->tile_blocks = polar_tile_blocks_per_sm() * ctx->sm_count;
     (void)nset;
     cudaEvent_t t0;
     ctx->stage_begin(0, &t0);
@@ -323,7 +325,13 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
         ctx->stage_end(3, ev);
         ctx->stage_begin(4, &ev);
-        if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) return false;
+        if (ctx->polar_tiles) {
+            if (!ctx->check("polar", launch_polar_tiles(w, ctx->fs_tiles.ptr, ctx->tile_capacity, cn,
+                                                        ctx->tile_blocks, ctx->stream)))
+                return false;
+        } else if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) {
+            return false;
+        }
         ctx->stage_end(4, ev);
         // Second pass, one block per point, over the points that passed the cell
         // budget or outgrew the first pass's scratch.
@@ -343,7 +351,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         if (!ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
         ctx->stage_end(4, ev);
         ctx->launches += 2;
-        ctx->launches += 4;
+        ctx->launches += 6;
     }
     return true;
 }

@@ -32,7 +32,7 @@ struct Context {
     Buffer fs_settings, fs_models, fs_raw_offset, fs_phases, fs_items, fs_out, fs_raw, fs_branches, fs_ld;
     Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
     Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
-    Buffer fs_cycles;
+    Buffer fs_cycles, fs_tiles;
     bool trig_ready = false;
     unsigned long long epoch = 0;
     int fs_warps = 0;          // persistent warps the scratch areas are sized for
@@ -51,6 +51,10 @@ struct Context {
     int queue_cap_big = 1 << 19;
     int hash_cap_big = 1 << 21;
     bool big_ready = false;
+    // Tile-parallel polar flood fill: table and FIFO capacity (power of two).
+    bool polar_tiles = true;
+    long long tile_capacity = 1 << 20;
+    int tile_blocks = 0;       // persistent flood blocks (0: occupancy x SMs)
     cudaStream_t own_stream = nullptr;  // the context's stream; `stream` may be a caller's
 
     // Optional per-stage kernel timing with CUDA events on the launch stream.
@@ -73,7 +77,7 @@ struct Context {
         for (Buffer* b : {&fs_settings, &fs_models, &fs_raw_offset, &fs_phases, &fs_items, &fs_out, &fs_raw,
                           &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
                           &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
-                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles})
+                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles})
             v.push_back(b);
         return v;
     }

@@ -94,6 +94,12 @@ cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, lon
                          int n_warps);
 cudaError_t launch_cartesian(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
 cudaError_t launch_polar(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
+// Tile-parallel polar flood fill of every polar point of the work lists
+// (first pass); points that do not fit go to the second-pass retry list.
+cudaError_t launch_polar_tiles(const FsWork& w, void* area, long long capacity, int max_items, int flood_blocks,
+                               cudaStream_t stream);
+size_t tile_bytes(long long capacity, int max_items);
+int polar_tile_blocks_per_sm();
 size_t seed_candidate_bytes_per_warp(int cand_cap);
 size_t cartesian_scratch_bytes(int row_cap, int seed_cap);
 size_t polar_scratch_bytes(int queue_cap, int hash_cap);

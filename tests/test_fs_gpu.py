@@ -152,9 +152,10 @@ def test_zero_radius_and_far_sources():
 
 @pytest.mark.parametrize("grid", ["cartesian", "polar"])
 def test_block_pass_matches_warp_pass(grid):
-    """Points moved to the second pass (one whole block per point, here every
-    point: cell budget 1) give bit-for-bit the results of the one-warp pass,
-    and both match the reference."""
+    """Every scan implementation gives bit-for-bit the same results, and they
+    match the reference: the first pass (Cartesian one warp per point; polar
+    tile-parallel flood fill, or one warp per point) and the second pass (one
+    block per point, here for every point: cell budget 1)."""
     import lcbinint_b200 as lb
     from lcbinint_b200 import _lib
     from oracle.oracle import default_settings
@@ -164,9 +165,11 @@ def test_block_pass_matches_warp_pass(grid):
     mode = {"cartesian": 1, "polar": 2}[grid]
     nbin = 45
     out = {}
+    runs = [(1 << 19, 1), (1 << 19, 0), (1, 0)]  # (cell budget, polar tiles)
     try:
-        for budget in (1 << 19, 1):
+        for budget, tiles in runs:
             assert ctx._L.lcbi_gpu_set_cell_budget(ctx.handle, budget) == 0
+            assert ctx._L.lcbi_gpu_set_polar_tiles(ctx.handle, tiles) == 0
             A_all, M_all, S_all = [], [], []
             for c in np.unique(cases[:, 5]):
                 sel = cases[:, 5] == c
@@ -177,13 +180,17 @@ def test_block_pass_matches_warp_pass(grid):
                 A_all.append(A)
                 M_all.append(m)
                 S_all.append(st)
-            out[budget] = (np.concatenate(A_all), np.concatenate(M_all), np.concatenate(S_all))
+            out[(budget, tiles)] = (np.concatenate(A_all), np.concatenate(M_all), np.concatenate(S_all))
     finally:
         ctx._L.lcbi_gpu_set_cell_budget(ctx.handle, 1 << 19)
-    (A0, M0, S0), (A1, M1, S1) = out[1 << 19], out[1]
-    assert (S0 == 0).all() and (S1 == 0).all()
-    assert np.array_equal(M0, M1)
-    assert np.array_equal(A0.view(np.int64), A1.view(np.int64)), _report(A1, A0)
+        ctx._L.lcbi_gpu_set_polar_tiles(ctx.handle, 1)
+    A0, M0, S0 = out[runs[0]]
+    assert (S0 == 0).all()
+    for key in runs[1:]:
+        A1, M1, S1 = out[key]
+        assert (S1 == 0).all()
+        assert np.array_equal(M0, M1)
+        assert np.array_equal(A0.view(np.int64), A1.view(np.int64)), (key, _report(A1, A0))
     R_all = []
     for c in np.unique(cases[:, 5]):
         sel = cases[:, 5] == c

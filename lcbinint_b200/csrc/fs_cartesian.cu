@@ -85,6 +85,10 @@ __device__ __forceinline__ int key_lookup(const RowScratch& R, int key, unsigned
     return -1;
 }
 
+// Rows [0, i] exist afterwards, rows that come into existence being zero (the
+// reference's vector resize).  Rows are zeroed ahead in batches of one per
+// thread: a row is only ever written after it exists, so the rows zeroed
+// ahead are still zero when they come into existence.
 template <int W>
 __device__ __forceinline__ void rows_ensure(RowScratch& R, int i)
 {
@@ -93,14 +97,15 @@ __device__ __forceinline__ void rows_ensure(RowScratch& R, int i)
         R.ovf = true;
         return;
     }
-    for (int r = R.hw + Grp<W>::rank(); r <= i; r += Grp<W>::N) {
+    const int end = min(R.cap, max(i + 1, R.hw + Grp<W>::N));
+    for (int r = R.hw + Grp<W>::rank(); r < end; r += Grp<W>::N) {
         R.xmin[r] = 0.0;
         R.xmax[r] = 0.0;
         R.ax[r] = 0.0;
         R.y[r] = 0.0;
         R.dys[r] = 0.0;
     }
-    R.hw = i + 1;
+    R.hw = end;
     Grp<W>::sync();
 }
 
@@ -267,6 +272,13 @@ __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a,
 }
 
 // cartesian_image_area_impl: one directional flood fill from `seed`.
+//
+// Every thread runs the same state machine on the same values, so the row
+// bounds the scan needs again (the previous row's xmin and xmax, the current
+// row's) are kept in registers instead of being read back from the scratch,
+// which only rank 0 writes and which is read back only after the scan.  The
+// row-key table slot of each row is fetched when the row starts, so its load
+// overlaps the row's lens-map evaluations.
 template <int W>
 __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, double dy, int& yi, int jsign)
 {
@@ -278,6 +290,21 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
     double ix = seed.x, iy = seed.y;
     double x0 = seed.x;
     int guard = 0;
+    // Row bounds in registers (see above); the scan's first row follows the
+    // predecessor row its caller prepared.  A row that ends with a count has
+    // had both of its bounds set during its own scan, so the current row's
+    // registers need no initial value.
+    double prev_xmin = 0.0, cur_xmin = 0.0, cur_xmax = 0.0;
+    rows_ensure<W>(R, yi);
+    if (R.ovf) return countall;
+    if (yi > 0) prev_xmin = R.xmin[yi - 1];
+    // Row-key table slot of the current row, fetched ahead; the slot rank 0
+    // wrote last is patched in, since the fetch may predate that write.
+    unsigned long long last_slot = ~0ull;
+    ulonglong2 last_entry = make_ulonglong2(0ull, 0ull);
+    int key = row_key(iy, inv_incr);
+    unsigned pre_h = key_hash(key, R.tmask);
+    ulonglong2 pre = R.table[pre_h];
     // Chunk: cells [0, N) from (chunk start, cy) along cdx; cidx is the next one to consume.
     bool have = false;
     int cidx = 0;
@@ -289,7 +316,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 return countall;
             }
             const bool want_cont = dx != incr && yi != 0;
-            const double thr = want_cont ? R.xmin[yi - 1] - dx : 0.0;
+            const double thr = want_cont ? prev_xmin - dx : 0.0;
             fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr);
             have = true;
             cidx = 0;
@@ -334,21 +361,30 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
         rows_ensure<W>(R, yi);
         if (R.ovf) return countall;
         if (dz2 <= C.rho2) {
-            if (dx == -incr && countx == 0.0) wset<W>(R.xmax, yi, ix - dx);
+            if (dx == -incr && countx == 0.0) {
+                cur_xmax = ix - dx;
+                wset<W>(R.xmax, yi, cur_xmax);
+            }
             countx += b;
             ++C.rays;
         } else if (dx == incr) {
-            if (last <= C.rho2) wset<W>(R.xmax, yi, ix);
+            if (last <= C.rho2) {
+                cur_xmax = ix;
+                wset<W>(R.xmax, yi, ix);
+            }
             dx = -incr;
             ix = x0;
-            wset<W>(R.xmin, yi, ix + dx);
+            cur_xmin = ix + dx;
+            wset<W>(R.xmin, yi, cur_xmin);
             have = false;
         } else {
-            if (last <= C.rho2) wset<W>(R.xmin, yi, ix);
-            Grp<W>::sync();
+            if (last <= C.rho2) {
+                cur_xmin = ix;
+                wset<W>(R.xmin, yi, ix);
+            }
             if (yi != 0 && countx == 0.0) {
                 rows_ensure<W>(R, yi - 1);
-                if (ix >= R.xmin[yi - 1] - dx) {
+                if (ix >= prev_xmin - dx) {
                     ix += dx;
                     continue;
                 }
@@ -359,39 +395,50 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
             wset<W>(R.dys, yi, dy);
             if (countx == 0.0) {
                 wset<W>(R.dys, yi, -dy);
-                Grp<W>::sync();
                 break;
             }
-            Grp<W>::sync();
             // Same-row overlap with an earlier row of this seed's scans (FSM:1990-1999).
-            const int key = row_key(iy, inv_incr);
+            if (pre_h == last_slot) pre = last_entry;
             unsigned slot;
-            int e = key_lookup(R, key, &slot);
-            if (slot == 0xffffffffu) {
-                R.ovf = true;
-                return countall;
+            int e;
+            if (pre.x != R.gen) {
+                slot = pre_h;
+                e = -1;
+            } else if ((int)(pre.y >> 32) == key) {
+                slot = pre_h;
+                e = (int)(pre.y & 0xffffffffull) - 1;
+            } else {
+                e = key_lookup(R, key, &slot);
+                if (slot == 0xffffffffu) {
+                    R.ovf = true;
+                    return countall;
+                }
             }
             const int head = e;
-            const double xmin_y = R.xmin[yi], xmax_y = R.xmax[yi];
             for (int hops = 0; e >= 0 && hops < R.cap; ++hops) {
-                if (xmin_y + incr < R.xmax[e] && xmax_y - incr > R.xmin[e]) return countall - countx;
+                if (cur_xmin + incr < R.xmax[e] && cur_xmax - incr > R.xmin[e]) return countall - countx;
                 e = R.next[e];
             }
+            last_slot = slot;
+            last_entry = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
+                                                    (unsigned long long)(unsigned)(yi + 1));
             if (Grp<W>::rank() == 0) {
                 R.next[yi] = head;
-                R.table[slot] = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
-                                                           (unsigned long long)(unsigned)(yi + 1));
+                R.table[slot] = last_entry;
             }
             ++yi;
             rows_ensure<W>(R, yi);
             if (R.ovf) return countall;
-            Grp<W>::sync();
             dx = incr;
-            x0 = R.xmax[yi - 1];
+            x0 = cur_xmax;
+            prev_xmin = cur_xmin;
             ix = x0 - dx;
             iy += dy;
             countx = 0.0;
             have = false;
+            key = row_key(iy, inv_incr);
+            pre_h = key_hash(key, R.tmask);
+            pre = R.table[pre_h];
         }
         ix += dx;
     }
@@ -696,7 +743,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
     }
 }
 
-__global__ void __launch_bounds__(128) cartesian_warp_kernel(FsWork w, unsigned long long epoch)
+__global__ void __launch_bounds__(128, 2) cartesian_warp_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<1> sh[4];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -704,7 +751,7 @@ __global__ void __launch_bounds__(128) cartesian_warp_kernel(FsWork w, unsigned 
     cartesian_body<1>(w, epoch, L, w.scratch + (long long)gw * w.scratch_per_warp, sh[warp_in_block()]);
 }
 
-__global__ void __launch_bounds__(32 * kBigWarps) cartesian_block_kernel(FsWork w, unsigned long long epoch)
+__global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<kBigWarps> sh;
     const CartList L{w.retry_cart, w.ir_count + 2, w.next_item + 3};

@@ -71,6 +71,14 @@ int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
  * fill spread over the whole GPU, 0 the one-warp-per-point segment flood fill.
  * Both count the same cells; results are the same.  No reference counterpart. */
 int lcbi_gpu_set_polar_tiles(lcbi_gpu_context *ctx, int enable);
+/* Device workspace of the finite-source scans (no reference counterpart):
+ * first-pass warps per SM (default 8; about 7 MB of scratch each), second-pass
+ * blocks (default 0: one per SM; about 100 MB each) and the polar tile table's
+ * capacity (a power of two, default 1048576 tiles of 400 B).  Smaller values
+ * trade speed for memory; results do not change.  A value <= 0 keeps the
+ * current setting, except second-pass blocks, where 0 means one per SM. */
+int lcbi_gpu_set_workspace(lcbi_gpu_context *ctx, int32_t warps_per_sm, int32_t second_pass_blocks,
+                           int64_t tile_capacity);
 /* Device-measured FP64 fused-multiply-add throughput of this GPU in TFLOP/s
  * (2 flop per FMA), the denominator of the FP64 roofline; no reference counterpart. */
 int lcbi_gpu_measure_fp64_peak(lcbi_gpu_context *ctx, double *tflops);

@@ -82,6 +82,8 @@ def _declare(L):
     L.lcbi_gpu_set_cell_budget.restype = C.c_int
     L.lcbi_gpu_set_polar_tiles.argtypes = [_vp, C.c_int]
     L.lcbi_gpu_set_polar_tiles.restype = C.c_int
+    L.lcbi_gpu_set_workspace.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int64]
+    L.lcbi_gpu_set_workspace.restype = C.c_int
     L.lcbi_gpu_last_item_cycles.argtypes = [_vp, C.c_int64, _vp]
     L.lcbi_gpu_last_item_cycles.restype = C.c_int
     L.lcbi_gpu_last_ray_counts.argtypes = [_vp, C.c_int64, _vp]

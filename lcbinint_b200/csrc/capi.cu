@@ -227,6 +227,21 @@ int lcbi_gpu_set_polar_tiles(lcbi_gpu_context* c, int enable)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_workspace(lcbi_gpu_context* c, int32_t warps_per_sm, int32_t second_pass_blocks,
+                           int64_t tile_capacity)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || second_pass_blocks < 0) return LCBI_INVALID_ARGUMENT;
+    if (tile_capacity > 0 && (tile_capacity & (tile_capacity - 1)) != 0) return LCBI_INVALID_ARGUMENT;
+    if (warps_per_sm > 0) ctx->warps_per_sm = warps_per_sm;  // the scratch is re-sized on the next call
+    if (second_pass_blocks != ctx->retry_blocks) {
+        ctx->retry_blocks = second_pass_blocks;
+        ctx->big_ready = false;
+    }
+    if (tile_capacity > 0) ctx->tile_capacity = tile_capacity;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_stage_times(const lcbi_gpu_context* c, double* ms, int64_t* launches, int32_t n)
 {
     const Context* ctx = reinterpret_cast<const Context*>(c);

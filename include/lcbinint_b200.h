@@ -96,6 +96,16 @@ int lcbi_gpu_binary_mag0(lcbi_gpu_context *ctx, int64_t n, const double *s, cons
                          const double *y1, const double *y2, double *A, int32_t *image_count,
                          int32_t *status, unsigned flags);
 
+/* Point-source magnification summed over the physical images of
+ * PointSourceMagnifier::binary_images
+ * (src/lcbinint/magnification/point_source_magnifier.cpp:723-778), in their
+ * order, as LensModel forms it (src/lcbinint/model/lens_model.cpp:209-216);
+ * image_count = number of those images (0 when s == 0 or q <= 0).  This can
+ * differ from lcbi_gpu_binary_mag0 in the last bits (another root selection). */
+int lcbi_gpu_binary_images_mag(lcbi_gpu_context *ctx, int64_t n, const double *s, const double *q,
+                               const double *y1, const double *y2, double *A, int32_t *image_count,
+                               unsigned flags);
+
 /* Point-source magnification plus the smoothness indicator the finite-source
  * decision tree uses.  Replaces PointSourceMagnifier::binary_mag0_with_derivatives
  * (src/lcbinint/magnification/point_source_magnifier.cpp:583-611). */
@@ -142,6 +152,8 @@ typedef struct lcbi_fs_point {
 
 #define LCBI_FS_PS_EXACT 1      /* point_source_magnification_is_exact */
 #define LCBI_FS_PS_ON_DEVICE 2  /* point_source_magnification = binary_mag0(s, q, y1, y2), on the GPU */
+#define LCBI_FS_SEED_HINTS 4    /* seed the inverse ray with the point images that map inside the source,
+                                   as LensModel passes them (src/lcbinint/model/lens_model.cpp:209-226) */
 
 /* A caustic model (s, q, caustic_bins), the key of the reference's caustic
  * cache (finite_source_magnifier.cpp:4014-4022). */
@@ -234,6 +246,124 @@ int lcbi_gpu_last_ray_counts(lcbi_gpu_context *ctx, int64_t n, uint64_t *rays);
 int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, double s, double q,
                                 int64_t n, const double *y1, const double *y2, const double *rho,
                                 lcbi_fs_result *results);
+
+/* ------------------------------------------------------------------ */
+/* The reference's own C ABI (include/lcbinint/lcbinint.h:15-136)       */
+/* ------------------------------------------------------------------ */
+
+/* Same types, field order, names and semantics as include/lcbinint/lcbinint.h,
+ * so a program written against the reference's header links against this
+ * library unchanged.  The magnification runs on the calling thread's current
+ * CUDA device, through a context kept per host thread.  Built: static binary
+ * lenses (q2 <= 0, no parallax, no xallarap, LCBI_ORBIT_STATIC) in both
+ * coordinate conventions, point and finite source, bit-identical to the
+ * reference.  Parameter sets that need the rest (triple lenses, parallax,
+ * xallarap, lens orbital motion) return LCBI_UNSUPPORTED, with the result
+ * filled as the reference fills it for unsupported input (NaN
+ * magnifications, the source position). */
+#ifndef LCBININT_H
+typedef enum lcbi_orbital_motion_mode {
+    LCBI_ORBIT_STATIC = 0,
+    LCBI_ORBIT_CIRCULAR = 1,
+    LCBI_ORBIT_KEPLER = 2
+} lcbi_orbital_motion_mode;
+
+typedef struct lcbi_params {
+    double t0;
+    double tE;
+    double umin;
+    double q;
+    double sep;
+    double theta;
+    double rho;
+    double omega;
+    double piEN;
+    double piEE;
+    double piEN_xa;
+    double piEE_xa;
+    double ra_xa;
+    double dec_xa;
+    double period_xa;
+    double ecc_xa;
+    double peri_xa;
+    double v_sep;
+    double q2;
+    double sep2;
+    double ang;
+    double ra;
+    double dec;
+    double earth_axis;
+    double tfix;
+    double obs_lat;
+    double obs_lon;
+    double limb_darkening_c;
+    double limb_darkening_d;
+    lcbi_orbital_motion_mode orbital_motion_mode;
+    double g1;
+    double g2;
+    double g3;
+    double lom_szs;
+    double lom_ar;
+    double xi_1;
+    double xi_2;
+    double omega_xa;
+    double inc_xa;
+    double phi_xa;
+} lcbi_params;
+
+typedef enum lcbi_xallarap_param_type {
+    LCBI_XALLARAP_NONE = 0,
+    LCBI_XALLARAP_ANGULAR_VELOCITY = 1,
+    LCBI_XALLARAP_ORBITAL_ELEMENTS = 2
+} lcbi_xallarap_param_type;
+
+typedef struct lcbi_options {
+    int parallax_mode;
+    int orbit_pair;
+    int center_of_mass;
+    int caustic_bins;
+    int source_bins;
+    int mode;                 /* 1 cartesian, 2 polar, 4 auto */
+    int vbm_compatible;       /* 0 original convention, 1 VBM convention */
+    lcbi_xallarap_param_type xallarap_param_type;
+    double grid_ratio;
+    int polar_source_bins;
+    double polar_grid_ratio;
+    double point_source_threshold;
+    double hexadecapole_threshold;
+    double adaptive_hex_threshold;
+    int adaptive_source_bins;
+    int max_source_bins;
+    double finite_source_tol;
+    double finite_source_reltol;
+} lcbi_options;
+
+typedef struct lcbi_result {
+    double magnification;
+    double point_source_magnification;
+    double finite_source_magnification;
+    double source_x;
+    double source_y;
+    int image_count;
+    double finite_source_error_estimate;
+    int finite_source_refinement_level;
+    int finite_source_converged;
+} lcbi_result;
+
+/* lcbinint.h:118-119: the reference's defaults. */
+lcbi_params lcbi_default_params(void);
+lcbi_options lcbi_default_options(void);
+/* lcbinint.h:121-126: one epoch (a batch of one). */
+lcbi_status lcbi_magnification(double time, const lcbi_params *params, const lcbi_options *options,
+                               lcbi_result *result);
+/* lcbinint.h:128-134: all epochs in one batch on the GPU; like the reference,
+ * results are written up to and including the first epoch that fails, whose
+ * status is returned. */
+lcbi_status lcbi_magnification_array(const double *times, int count, const lcbi_params *params,
+                                     const lcbi_options *options, lcbi_result *results);
+/* lcbinint.h:136. */
+const char *lcbi_status_string(lcbi_status status);
+#endif
 
 #ifdef __cplusplus
 }

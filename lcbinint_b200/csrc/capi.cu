@@ -301,6 +301,35 @@ int lcbi_gpu_binary_mag0(lcbi_gpu_context* c, int64_t n, const double* s, const 
     return LCBI_OK;
 }
 
+int lcbi_gpu_binary_images_mag(lcbi_gpu_context* c, int64_t n, const double* s, const double* q, const double* y1,
+                               const double* y2, double* A, int32_t* image_count, unsigned flags)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!s || !q || !y1 || !y2 || !A) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
+    const size_t N = static_cast<size_t>(n);
+    const double *ds, *dq, *dy1, *dy2;
+    double* dA;
+    int* dn;
+    if (!ctx->stage_in(ctx->in[0], s, N, dev, &ds) || !ctx->stage_in(ctx->in[1], q, N, dev, &dq) ||
+        !ctx->stage_in(ctx->in[2], y1, N, dev, &dy1) || !ctx->stage_in(ctx->in[3], y2, N, dev, &dy2) ||
+        !ctx->stage_out(ctx->out[0], A, N, dev, &dA) ||
+        !ctx->stage_out(ctx->out[1], reinterpret_cast<int*>(image_count), N, dev, &dn))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("ps_images_kernel", lcbi::launch_ps_images(ds, dq, dy1, dy2, dA, dn, n, ctx->sm_count,
+                                                               ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    if (!ctx->copy_back(A, dA, N, dev) || !ctx->copy_back(reinterpret_cast<int*>(image_count), dn, N, dev) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_binary_mag0_derivatives(lcbi_gpu_context* c, int64_t n, const double* s, const double* q,
                                      const double* y1, const double* y2, double* A, int32_t* image_count,
                                      double* indicator, unsigned flags)

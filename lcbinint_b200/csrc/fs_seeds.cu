@@ -344,18 +344,29 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
         S.sh = sh;
 
         // Point images at the source centre (binary_images, point_source_magnifier.cpp:723-737).
+        // As seed hints (LensModel, lens_model.cpp:209-226) only the images that
+        // map inside the source are kept (append_valid_seed, FSM:1430-1447), all
+        // of them if none does (FSM:1722-1727).
         {
-            double px = 0.0, py = 0.0;
             int cnt = 0;
             if (lane_id() == 0 && item.s != 0.0 && item.q > 0.0) {
                 const BinaryGeom g = make_geom(item.s, item.q, item.x, item.y);
                 dc pos[5];
                 double res[5], det[5];
-                cnt = image_candidates(g, pos, res, det);
-                for (int i = 0; i < cnt; ++i) S.seeds[i] = P2{pos[i].re, pos[i].im};
+                const int all = image_candidates(g, pos, res, det);
+                if (item.flags & kItemSeedHints) {
+                    for (int i = 0; i < all; ++i) {
+                        if (!(S.rho > 0.0)) break;
+                        const P2 mp = map_real(S.m, pos[i].re, pos[i].im);
+                        if (dist2(mp, S.src) > S.rho2 * (1.0 + 1.0e-8)) continue;
+                        S.seeds[cnt++] = P2{pos[i].re, pos[i].im};
+                    }
+                }
+                if (cnt == 0) {
+                    for (int i = 0; i < all; ++i) S.seeds[i] = P2{pos[i].re, pos[i].im};
+                    cnt = all;
+                }
             }
-            (void)px;
-            (void)py;
             S.n = shfl_i(cnt, 0);
             __syncwarp();
         }

@@ -20,6 +20,7 @@ struct FsItem {
 enum : int {
     kItemPsExact = 1,     // point_source_magnification_is_exact (hexadecapole reuses a_ps)
     kItemPsOnDevice = 2,  // a_ps = binary_mag0(s, q, x, y), computed by the decision kernel
+    kItemSeedHints = 4,   // the point images are seed hints, kept only if they map inside the source
 };
 
 // Per-item outputs.

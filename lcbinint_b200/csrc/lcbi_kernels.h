@@ -12,4 +12,7 @@ cudaError_t launch_ps_batch(const double* s, const double* q, const double* y1, 
 cudaError_t launch_ps_deriv(const double* s, const double* q, const double* y1, const double* y2, double* A,
                             int* nimg, double* indicator, long long n, int sm_count, cudaStream_t stream);
 
+cudaError_t launch_ps_images(const double* s, const double* q, const double* y1, const double* y2, double* A,
+                             int* nimg, long long n, int sm_count, cudaStream_t stream);
+
 } // namespace lcbi

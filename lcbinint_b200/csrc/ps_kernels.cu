@@ -51,6 +51,42 @@ __global__ void __launch_bounds__(128) ps_deriv_kernel(const double* __restrict_
     }
 }
 
+// Magnification summed over the physical images of binary_images
+// (point_source_magnifier.cpp:723-778) in their residual order, as LensModel
+// forms the finite-source decision's point-source value
+// (lens_model.cpp:209-216).
+__global__ void __launch_bounds__(128) ps_images_kernel(const double* __restrict__ s, const double* __restrict__ q,
+                                                       const double* __restrict__ y1, const double* __restrict__ y2,
+                                                       double* __restrict__ A, int* __restrict__ nimg, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double a = 0.0;
+        int cnt = 0;
+        if (s[i] != 0.0 && q[i] > 0.0) {
+            const BinaryGeom g = make_geom(s[i], q[i], y1[i], y2[i]);
+            dc pos[5];
+            double res[5], det[5];
+            cnt = image_candidates(g, pos, res, det);
+            for (int k = 0; k < cnt; ++k) a += 1.0 / fabs(det[k]);
+        }
+        A[i] = a;
+        if (nimg) nimg[i] = cnt;
+    }
+}
+
+cudaError_t launch_ps_images(const double* s, const double* q, const double* y1, const double* y2, double* A,
+                             int* nimg, long long n, int sm_count, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const int threads = 128;
+    long long blocks = (n + threads - 1) / threads;
+    const long long cap = (long long)sm_count * 16;
+    if (blocks > cap) blocks = cap;
+    ps_images_kernel<<<(unsigned)blocks, threads, 0, stream>>>(s, q, y1, y2, A, nimg, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ps_batch(const double* s, const double* q, const double* y1, const double* y2, double* A,
                             int* nimg, int* status, long long n, int sm_count, cudaStream_t stream)
 {

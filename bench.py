@@ -226,6 +226,24 @@ def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
 # --------------------------------------------------------------------------- main
 
 
+def reduce_over_ranks(maxes, sums, world, device):
+    """Across the ranks: the max of each entry of `maxes` (timings: the job is
+    as slow as its slowest rank) and the sum of each entry of `sums` (points
+    and cells processed), so that a replica job's throughput is the work of
+    all ranks over the slowest rank's time."""
+    maxes = [float(v) for v in maxes]
+    sums = [float(v) for v in sums]
+    if world == 1:
+        return maxes, sums
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(maxes, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor(sums, dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return t.cpu().tolist(), c.cpu().tolist()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -278,7 +296,7 @@ def main():
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device(f"cuda:{local_rank}")
     torch.cuda.set_device(dev)
 
@@ -356,19 +374,13 @@ def main():
     rays = np.zeros(n, dtype=np.uint64)
     L.lcbi_gpu_last_ray_counts(ctx.handle, n, _lib.ptr(rays))
     res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=FS_RESULT_DTYPE)
-    if world > 1:
-        t = torch.tensor([my_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        max_ms = float(t.item())
-    else:
-        max_ms = my_ms
-    ms_per_step = max_ms / args.steps
-    value = world * n / (ms_per_step * 1e-3)
 
     # end to end: host arrays through the public C ABI (planning, H2D copies,
     # kernels, D2H of the results), wall-clocked per step
     for _ in range(2):
         step_e2e()
+    if world > 1:
+        torch.distributed.barrier()
     e2e_s = 0.0
     for _ in range(args.steps):
         flush_l2(flush)
@@ -376,6 +388,9 @@ def main():
         t1 = time.perf_counter()
         step_e2e()
         e2e_s += time.perf_counter() - t1
+    (max_ms, max_e2e_s), (n_all, rays_all) = reduce_over_ranks([my_ms, e2e_s], [n, float(rays.sum())], world, dev)
+    ms_per_step = max_ms / args.steps
+    value = n_all / (ms_per_step * 1e-3)
 
     peak = ctypes_double()
     L.lcbi_gpu_measure_fp64_peak(ctx.handle, peak.ref())
@@ -401,11 +416,11 @@ def main():
         "metric": METRIC, "value": value, "unit": "magnifications/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
-        "rays_per_s": world * rays_total / (ms_per_step * 1e-3),
+        "rays_per_s": rays_all / (ms_per_step * 1e-3),
         "methods": {"cartesian": int(cart.sum()), "polar": int(polar_m.sum())},
         "status_ok": int((res["status"] == 0).sum()),
         "roofline": roofline,
-        "e2e": {"value": n * args.steps / e2e_s, "unit": "magnifications/s",
+        "e2e": {"value": n_all * args.steps / max_e2e_s, "unit": "magnifications/s",
                 "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(res_host.nbytes)},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),

@@ -223,6 +223,211 @@ def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
     return n / wall, n, wall
 
 
+# --------------------------------------------------------------------------- configs 1 and 2
+
+
+def ps_batch_workload(n=1_000_000, seed=0):
+    """Point-source batch (config 2): y uniform in [-1.5, 1.5]^2, s log-U[0.3, 3],
+    q log-U[1e-5, 1] in the core convention, per point."""
+    rng = np.random.default_rng(seed)
+    s = np.exp(rng.uniform(np.log(0.3), np.log(3.0), n))
+    q = np.exp(rng.uniform(np.log(1e-5), 0.0, n))
+    y1 = rng.uniform(-1.5, 1.5, n)
+    y2 = rng.uniform(-1.5, 1.5, n)
+    return s, q, y1, y2
+
+
+LC_PARAMS = dict(t0=0.0, tE=1.0, u0=-0.01, alpha=0.5, s=0.95, q=1e-2, rho=5e-3)
+
+
+def _ref_ps_worker(args):
+    s, q, y1, y2, reps = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Reference
+    ref = Reference()
+    t = time.perf_counter()
+    for _ in range(reps):
+        ref.binary_mag0(s, q, y1, y2)
+    return time.perf_counter() - t
+
+
+def cpu_ps_rate(s, q, y1, y2, n_procs, target_seconds):
+    """Point-source magnifications/s of the reference, one process per core,
+    each repeating its share of the batch until about target_seconds."""
+    import multiprocessing as mp
+    share = [(s[k::n_procs], q[k::n_procs], y1[k::n_procs], y2[k::n_procs]) for k in range(n_procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n_procs) as pool:
+        cal = max(pool.map(_ref_ps_worker, [(a, b, c, d, 1) for a, b, c, d in share]))
+        reps = int(max(1, min(50, target_seconds / max(cal, 1e-3))))
+        t0 = time.perf_counter()
+        pool.map(_ref_ps_worker, [(a, b, c, d, reps) for a, b, c, d in share])
+        wall = time.perf_counter() - t0
+    n = reps * s.size
+    return n / wall, n, wall
+
+
+def cpu_light_curve_rate(target_seconds):
+    """The reference's own light-curve path (one curve, one core) on config 1."""
+    from oracle.oracle import Reference, default_settings
+    ref = Reference()
+    times = np.linspace(-0.5, 0.5, 200)
+    st = default_settings(source_bins=50, finite_mode=1, limb_darkening_c=0.5)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        ref.light_curve_static(st, times, **LC_PARAMS)
+        n += times.size
+        if time.perf_counter() - t0 > target_seconds:
+            break
+    wall = time.perf_counter() - t0
+    return n / wall, n, wall
+
+
+def run_other_workload(args, world, rank, local_rank, ncores):
+    """Configs 2 (ps_batch) and 1 (light_curve): same JSON line as fs_batch."""
+    common = {"metric": METRIC, "unit": "magnifications/s", "steps": args.steps, "warmup": args.warmup,
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+              "data": "synthetic"}
+    if args.workload == "ps_batch":
+        config = {"workload": "ps_batch: 1e6 point-source magnifications, y U[-1.5,1.5]^2, s log-U[0.3,3], "
+                              "q log-U[1e-5,1]", "points": 1_000_000, "l2": "flushed between steps (256 MB write)",
+                  "parallelism": f"replicas x{world}"}
+    else:
+        config = {"workload": "light_curve: README curve, 200 epochs, t0=0 tE=1 u0=-0.01 alpha=0.5 s=0.95 "
+                              "q=1e-2 rho=5e-3, linear LD 0.5, Cartesian nbin 50, VBM coordinates",
+                  "points": 200, "l2": "inputs and workspaces under 1 MB; not flushed (one curve)",
+                  "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        if args.workload == "ps_batch":
+            s, q, y1, y2 = ps_batch_workload()
+            rate, n, wall = cpu_ps_rate(s, q, y1, y2, ncores, max(2.0, args.cpu_seconds / 2))
+            cores, sample = ncores, f"{n} solves ({n // s.size} passes over the batch), {wall:.1f} s on {ncores} processes"
+        else:
+            rate, n, wall = cpu_light_curve_rate(max(2.0, args.cpu_seconds / 4))
+            cores, sample = 1, f"{n // 200} evaluations of the 200-epoch curve, {wall:.1f} s, one process"
+        out = dict(common, impl="reference", value=rate, n_gpus=args.gpus, ms_per_step=1e3 * wall * 200 / n
+                   if args.workload == "light_curve" else 1e3 * wall * 1e6 / n, config=config,
+                   cpu_baseline={"value": rate, "unit": "magnifications/s", "cores": cores, "kind": "reference",
+                                 "sample": sample},
+                   e2e={"value": rate, "unit": "magnifications/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(out))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    import lcbinint_b200 as lb
+    from lcbinint_b200 import _lib
+    ctx = lb.context(local_rank)
+    L = ctx._L
+    stream = torch.cuda.current_stream(dev)
+    L.lcbi_gpu_set_stream(ctx.handle, stream.cuda_stream)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    if args.workload == "ps_batch":
+        host = [np.ascontiguousarray(a) for a in ps_batch_workload(seed=rank)]
+        n = host[0].size
+        d_in = [torch.from_numpy(a).to(dev) for a in host]
+        d_A = torch.empty(n, dtype=torch.float64, device=dev)
+        d_n = torch.empty(n, dtype=torch.int32, device=dev)
+        pinned = [torch.from_numpy(a).pin_memory() for a in host]
+        h_A = torch.empty(n, dtype=torch.float64).pin_memory()
+        h_n = torch.empty(n, dtype=torch.int32).pin_memory()
+
+        def step_device():
+            rc = L.lcbi_gpu_binary_mag0(ctx.handle, n, *[t.data_ptr() for t in d_in], d_A.data_ptr(),
+                                        d_n.data_ptr(), None, 1)
+            ctx.check(rc, "lcbi_gpu_binary_mag0")
+
+        def step_e2e():
+            rc = L.lcbi_gpu_binary_mag0(ctx.handle, n, *[t.data_ptr() for t in pinned], h_A.data_ptr(),
+                                        h_n.data_ptr(), None, 0)
+            ctx.check(rc, "lcbi_gpu_binary_mag0")
+        h2d, d2h = sum(a.nbytes for a in host), n * 12
+        flush_between = True
+    else:
+        P = np.array([[LC_PARAMS[k] for k in ("t0", "tE", "u0", "alpha", "s", "q", "rho")]], dtype=np.float64)
+        times = np.linspace(-0.5, 0.5, 200)
+        n = times.size
+        opt = lb.Options(inverse_ray_grid="cartesian", nbin=50)
+        st = opt.fs_settings(lb.LimbDarkening.linear(0.5))
+        first = np.zeros(1, dtype=np.int64)
+        cnt = np.array([n], dtype=np.int32)
+        A = np.empty(n)
+
+        def step_device():
+            rc = L.lcbi_gpu_light_curves(ctx.handle, __import__("ctypes").byref(st), 1, _lib.ptr(P),
+                                         _lib.ptr(first), _lib.ptr(cnt), _lib.ptr(times), n, _lib.ptr(A), None,
+                                         None)
+            ctx.check(rc, "lcbi_gpu_light_curves")
+        step_e2e = step_device
+        h2d, d2h = times.nbytes + P.nbytes, A.nbytes
+        flush_between = False
+    for _ in range(args.warmup):
+        if flush_between:
+            flush_l2(flush)
+        step_device()
+    torch.cuda.synchronize(dev)
+    launches0 = ctx.launches
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            if flush_between:
+                flush_l2(flush)
+            ev0[k].record(stream)
+            step_device()
+            ev1[k].record(stream)
+        torch.cuda.synchronize(dev)
+    my_ms = float(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1)))
+    launches = ctx.launches - launches0
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        if flush_between:
+            flush_l2(flush)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        step_e2e()
+        e2e_s += time.perf_counter() - t1
+    (max_ms, max_e2e), (n_all,) = reduce_over_ranks([my_ms, e2e_s], [n], world, dev)
+    ms_per_step = max_ms / args.steps
+    peak = ctypes_double()
+    L.lcbi_gpu_measure_fp64_peak(ctx.handle, peak.ref())
+    out = dict(common, value=n_all / (ms_per_step * 1e-3), n_gpus=world, ms_per_step=ms_per_step, config=config,
+               e2e={"value": n_all * args.steps / max_e2e, "unit": "magnifications/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+               gpu_launches=int(launches), clocks=clocks.summary())
+    if args.workload == "ps_batch":
+        achieved = n * F_PS / (ms_per_step * 1e-3) / 1e12
+        out["roofline"] = {"bound": "fp64", "kernel": "ps_batch_kernel", "achieved": achieved, "peak": peak.value,
+                           "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
+                           "traffic": None, "flop_per_solve": F_PS,
+                           "peak_source": "device-measured FP64 FMA loop (lcbi_gpu_measure_fp64_peak)"}
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        if args.workload == "ps_batch":
+            rate, nn, wall = cpu_ps_rate(*host, ncores, args.cpu_seconds / 2)
+            out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                                   "sample": f"{nn} solves, {wall:.1f} s on {ncores} processes"}
+        else:
+            rate, nn, wall = cpu_light_curve_rate(args.cpu_seconds / 4)
+            out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": 1, "kind": "reference",
+                                   "sample": f"{nn // 200} curves, {wall:.1f} s, one process"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 # --------------------------------------------------------------------------- main
 
 
@@ -250,7 +455,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch"])
+    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch", "ps_batch", "light_curve"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,
@@ -262,6 +467,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
+    if args.workload != "fs_batch":
+        run_other_workload(args, world, rank, local_rank, ncores)
+        return
     rows = fs_batch_workload(seed=1 + rank)
     if args.points > 0:
         rows = rows[np.random.default_rng(5).permutation(len(rows))[: args.points]]

@@ -240,6 +240,50 @@ def ps_batch_workload(n=1_000_000, seed=0):
 LC_PARAMS = dict(t0=0.0, tE=1.0, u0=-0.01, alpha=0.5, s=0.95, q=1e-2, rho=5e-3)
 
 
+def adjoint_workload(seed=2, n_models=256, n_epochs=500):
+    """Config 4: models drawn as in config 3, epochs uniform over t0 +- 2 tE.
+    Returns params (M, 8) = (t0, tE, u0, alpha, s, q, rho, Gamma) and times (M, K)."""
+    rng = np.random.default_rng(seed)
+    P = np.empty((n_models, 8))
+    P[:, 0] = 0.0
+    P[:, 1] = 20.0
+    P[:, 2] = rng.uniform(-0.2, 0.2, n_models)
+    P[:, 3] = rng.uniform(0.0, 2.0 * np.pi, n_models)
+    P[:, 4] = np.exp(rng.uniform(np.log(0.3), np.log(3.0), n_models))
+    P[:, 5] = np.exp(rng.uniform(np.log(1e-5), 0.0, n_models))
+    P[:, 6] = np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), n_models))
+    P[:, 7] = rng.uniform(0.0, 0.8, n_models)
+    T = P[:, :1] + P[:, 1:2] * rng.uniform(-2.0, 2.0, (n_models, n_epochs))
+    return P, np.sort(T, axis=1)
+
+
+def _ref_lc_worker(args):
+    P, T = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Reference, default_settings
+    ref = Reference()
+    t = time.perf_counter()
+    for p, times in zip(P, T):
+        st = default_settings(source_bins=50, finite_mode=4, limb_darkening_c=float(p[7]))
+        ref.light_curve_static(st, times, t0=p[0], tE=p[1], u0=p[2], alpha=p[3], s=p[4], q=p[5], rho=p[6])
+    return time.perf_counter() - t
+
+
+def cpu_adjoint_rate(P, T, n_procs, n_models):
+    """The reference's forward on a sample of models, one process per core; a
+    central finite-difference gradient in 8 parameters costs 17 forwards."""
+    import multiprocessing as mp
+    idx = np.random.default_rng(11).permutation(len(P))[:n_models]
+    chunks = [(P[idx[k::n_procs]], T[idx[k::n_procs]]) for k in range(n_procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n_procs) as pool:
+        t0 = time.perf_counter()
+        pool.map(_ref_lc_worker, chunks)
+        wall = time.perf_counter() - t0
+    n = len(idx) * T.shape[1]
+    return n / wall / 17.0, n, wall
+
+
 def _ref_ps_worker(args):
     s, q, y1, y2, reps = args
     sys.path.insert(0, str(ROOT))
@@ -297,6 +341,9 @@ def run_other_workload(args, world, rank, local_rank, ncores):
                               "q=1e-2 rho=5e-3, linear LD 0.5, Cartesian nbin 50, VBM coordinates",
                   "points": 200, "l2": "inputs and workspaces under 1 MB; not flushed (one curve)",
                   "parallelism": f"replicas x{world}"}
+    if args.workload == "adjoint":
+        run_adjoint(args, world, rank, local_rank, ncores, common)
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -428,6 +475,108 @@ def run_other_workload(args, world, rank, local_rank, ncores):
         print(json.dumps(out))
 
 
+def run_adjoint(args, world, rank, local_rank, ncores, common):
+    """Config 4: magnifications and their gradients in (t0, tE, u0, alpha, s,
+    q, rho, Gamma) for 256 models x 500 epochs through the library's adjoint
+    (lcbi_gpu_light_curves_grad), against the forward alone, against a plain
+    GPU forward of one point per call with central finite differences (17
+    forwards per point), and against the reference's CPU forward with the same
+    finite differences."""
+    P, T = adjoint_workload(seed=2 + rank)
+    M, K = T.shape
+    n = M * K
+    config = {"workload": "adjoint: 256 models x 500 epochs (config-3 model distribution, t0 +- 2 tE), auto "
+                          "decision tree, nbin 50, dA/d(t0, tE, u0, alpha, s, q, rho, Gamma)",
+              "points": n, "l2": "not flushed (inputs and results under 11 MB; workspaces reused)",
+              "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rate, nn, wall = cpu_adjoint_rate(P, T, ncores, max(ncores, 32))
+        out = dict(common, impl="reference", value=rate, n_gpus=args.gpus, ms_per_step=1e3 * n / rate,
+                   config=config,
+                   cpu_baseline={"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                                 "sample": f"forward on {nn} epochs of {nn // K} models, {wall:.1f} s; "
+                                           "x17 for central differences in 8 parameters"},
+                   e2e={"value": rate, "unit": "magnifications/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(out))
+        return
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    import lcbinint_b200 as lb
+    from lcbinint_b200 import _lib
+    from lcbinint_b200.autograd import light_curves_with_grad
+    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, PS_EXACT, PS_ON_DEVICE, LcbiStructs
+    ctx = lb.context(local_rank)
+    L = ctx._L
+    for _ in range(args.warmup):
+        light_curves_with_grad(P, T, device=local_rank)
+        light_curves_with_grad(P, T, device=local_rank, with_grad=False)
+    launches0 = ctx.launches
+    with ClockSampler(local_rank) as clocks:
+        tg = tf = 0.0
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            A, dA, method, status = light_curves_with_grad(P, T, device=local_rank)
+            tg += time.perf_counter() - t1
+            t1 = time.perf_counter()
+            light_curves_with_grad(P, T, device=local_rank, with_grad=False)
+            tf += time.perf_counter() - t1
+    launches = (ctx.launches - launches0) // 2
+    # Plain GPU baseline: one point per call (positions as the light curves
+    # form them), 17 calls per point for central differences.
+    rng = np.random.default_rng(3)
+    sample = rng.integers(0, n, 64)
+    opt = lb.Options()
+    st_cache = {}
+    pts = np.zeros(1, dtype=FS_POINT_DTYPE)
+    res = np.zeros(1, dtype=FS_RESULT_DTYPE)
+    t_plain = 0.0
+    for k in sample:
+        m, e = divmod(int(k), K)
+        t0, tE, u0, al, s_, q_, rho, gam = P[m]
+        tau = (T[m, e] - t0) * (1.0 / tE)
+        g = float(gam)
+        if g not in st_cache:
+            st_cache[g] = opt.fs_settings(lb.LimbDarkening.linear(g))
+        st = st_cache[g]
+        pts[0] = (s_, 1.0 / q_, tau * math.cos(al) - u0 * math.sin(al), tau * math.sin(al) + u0 * math.cos(al),
+                  abs(rho), 0.0, 0, 0, PS_EXACT | PS_ON_DEVICE, 0)
+        t1 = time.perf_counter()
+        rc = L.lcbi_gpu_binary_mag(ctx.handle, __import__("ctypes").byref(st), 1, None, 0, 1, pts.ctypes.data,
+                                   res.ctypes.data, 0)
+        t_plain += time.perf_counter() - t1
+        ctx.check(rc, "lcbi_gpu_binary_mag")
+    plain_rate = len(sample) / t_plain / 17.0
+    (max_g, max_f), (n_all,) = reduce_over_ranks([tg, tf], [n], world, dev)
+    value = n_all * args.steps / max_g
+    out = dict(common, value=value, n_gpus=world, ms_per_step=1e3 * max_g / args.steps, config=config,
+               fwd_grad_over_fwd=max_g / max_f,
+               forward_only={"value": n_all * args.steps / max_f, "unit": "magnifications/s"},
+               plain_gpu_fd={"value": plain_rate, "unit": "magnifications/s",
+                             "how": "one point per lcbi_gpu_binary_mag call, 17 calls per gradient, 64 points"},
+               speedup_vs_plain_gpu_fd=value / plain_rate,
+               methods={str(k): int((method == k).sum()) for k in range(4)},
+               status_ok=int((status == 0).sum()), grad_finite=int(np.isfinite(dA).all(axis=2).sum()),
+               e2e={"value": value, "unit": "magnifications/s", "h2d_bytes_per_step": int(P.nbytes + T.nbytes),
+                    "d2h_bytes_per_step": int(n * 8 * 9)},
+               gpu_launches=int(launches), clocks=clocks.summary())
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, nn, wall = cpu_adjoint_rate(P, T, ncores, max(ncores, 32))
+        out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                               "sample": f"forward on {nn} epochs of {nn // K} models, {wall:.1f} s on {ncores} "
+                                         "processes; x17 for central differences in 8 parameters"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 # --------------------------------------------------------------------------- main
 
 
@@ -455,7 +604,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch", "ps_batch", "light_curve"])
+    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch", "ps_batch", "light_curve", "adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,

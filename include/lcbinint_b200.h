@@ -64,8 +64,9 @@ int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles)
  * whose Cartesian or polar scan passes `cells` lattice cells on its one warp
  * is moved to a second pass that runs it on a whole block with a larger
  * scratch.  0 disables the move (points then change pass only when they
- * outgrow the per-warp scratch); the default is 524288.  Results are the same
- * for every value. */
+ * outgrow the per-warp scratch); the default is 524288, and 1 (every point on
+ * a block) for calls of at most 4 points per SM until this is called.  Results
+ * are the same for every value. */
 int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
 /* Polar inverse ray in the first pass: 1 (default) the tile-parallel flood
  * fill spread over the whole GPU, 0 the one-warp-per-point segment flood fill.
@@ -208,6 +209,33 @@ int lcbi_gpu_binary_inverse_ray(lcbi_gpu_context *ctx, const lcbi_fs_settings *s
 int lcbi_gpu_light_curves(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_models,
                           const double *params, const int64_t *first, const int32_t *count,
                           const double *times, int64_t n_times, double *A, int32_t *method, int32_t *status);
+
+/* Adjoint (no reference counterpart: the reference has no gradient; its
+ * users difference the forward).  As lcbi_gpu_binary_mag, plus grads[8 * n]:
+ * per point dA/d(y1, y2, s, q, rho, c) in the point's own parameters (core
+ * convention, linear limb-darkening coefficient c), then the value that was
+ * differentiated and the method.  Point source and hexadecapole: exact
+ * derivatives of the forward's closed forms (implicit differentiation of the
+ * lens-equation roots).  Inverse ray: derivatives of the continuum
+ * magnification the lattice approximates -- image-boundary contour integrals
+ * at rho and six Gauss-Legendre radii, which carry the limb-darkening term
+ * without its interior singularity, on a lattice of rho/48 cells (slot 6 holds
+ * the continuum value).  Quadratic limb darkening (d != 0) gives NaN for
+ * inverse-ray points. */
+int lcbi_gpu_binary_mag_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_settings,
+                             const lcbi_lens_model *models, int32_t n_models, int64_t n,
+                             const lcbi_fs_point *points, lcbi_fs_result *results, double *grads,
+                             unsigned flags);
+
+/* Light curves with gradients: params[m] = {t0, tE, u0, alpha, s, q, rho,
+ * Gamma} (VBM convention, Gamma the linear limb-darkening coefficient, which
+ * replaces settings->limb_darkening_c per model); A[n_times] and, if dA is not
+ * NULL, dA[8 * n_times] = dA/d(t0, tE, u0, alpha, s, q, rho, Gamma) per epoch.
+ * The forward is lcbi_gpu_light_curves' (same magnifications). */
+int lcbi_gpu_light_curves_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_models,
+                               const double *params, const int64_t *first, const int32_t *count,
+                               const double *times, int64_t n_times, double *A, double *dA, int32_t *method,
+                               int32_t *status);
 
 /* Lattice cells counted by the last finite-source call (one count per point,
  * cells whose centre maps inside the source disk), for ray-throughput

@@ -84,6 +84,10 @@ def _declare(L):
     L.lcbi_gpu_set_polar_tiles.restype = C.c_int
     L.lcbi_gpu_set_workspace.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int64]
     L.lcbi_gpu_set_workspace.restype = C.c_int
+    L.lcbi_gpu_binary_mag_grad.argtypes = [_vp, _vp, C.c_int32, _vp, C.c_int32, C.c_int64, _vp, _vp, _vp, C.c_uint]
+    L.lcbi_gpu_binary_mag_grad.restype = C.c_int
+    L.lcbi_gpu_light_curves_grad.argtypes = [_vp, _vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp]
+    L.lcbi_gpu_light_curves_grad.restype = C.c_int
     L.lcbi_gpu_last_item_cycles.argtypes = [_vp, C.c_int64, _vp]
     L.lcbi_gpu_last_item_cycles.restype = C.c_int
     L.lcbi_gpu_last_ray_counts.argtypes = [_vp, C.c_int64, _vp]

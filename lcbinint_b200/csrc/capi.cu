@@ -216,6 +216,7 @@ int lcbi_gpu_set_cell_budget(lcbi_gpu_context* c, int64_t cells)
     Context* ctx = reinterpret_cast<Context*>(c);
     if (!ctx || cells < 0) return LCBI_INVALID_ARGUMENT;
     ctx->cell_budget = cells;
+    ctx->cell_budget_set = true;
     return LCBI_OK;
 }
 

@@ -208,7 +208,7 @@ bool upload(Context* ctx, Buffer& b, const std::vector<T>& v)
 
 // Runs the pipeline on device-resident items (ctx->fs_items) and writes device
 // results to ctx->fs_out.  Everything is asynchronous on ctx->stream.
-bool run_pipeline(Context* ctx, const Plan& plan, long long n)
+bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = nullptr)
 {
     // Candidate lists of the caustic-branch seed probes hold one entry per sampled point.
     if (4 * plan.max_bins > ctx->cand_cap) {
@@ -295,7 +295,9 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         w.retry_polar = w.retry_cart + kChunk;
         w.cand_cap = ctx->cand_cap;
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
-        w.cell_budget = ctx->cell_budget;
+        // A batch too small to fill the GPU with one warp per point (a single
+        // light curve, say) runs every inverse-ray point on a whole block.
+        w.cell_budget = (!ctx->cell_budget_set && cn <= 4 * ctx->sm_count) ? 1 : ctx->cell_budget;
         if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
         cudaEvent_t ev;
         ctx->stage_begin(1, &ev);
@@ -352,6 +354,15 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n)
         ctx->stage_end(4, ev);
         ctx->launches += 2;
         ctx->launches += 6;
+        if (grads) {
+            if (!ctx->ensure(ctx->fs_grad_tiles, grad_tile_bytes(ctx->tile_capacity, kChunk))) return false;
+            if (ctx->grad_blocks == 0) ctx->grad_blocks = grad_flood_blocks_per_sm() * ctx->sm_count;
+            if (!ctx->check("gradient", launch_grad(w, ctx->fs_grad_tiles.ptr, ctx->tile_capacity, cn,
+                                                    ctx->grad_blocks, ctx->grad_bins, ctx->sm_count, grads + c0 * 8,
+                                                    ctx->stream)))
+                return false;
+            ctx->launches += 6;
+        }
     }
     return true;
 }
@@ -382,11 +393,39 @@ using namespace lcbi;
 
 extern "C" {
 
+namespace lcbi {
+namespace {
+int binary_mag_impl(Context* ctx, const lcbi_fs_settings* settings, int32_t n_settings, const lcbi_lens_model* models,
+                    int32_t n_models, int64_t n, const lcbi_fs_point* points, lcbi_fs_result* results, double* grads,
+                    unsigned flags);
+}
+} // namespace lcbi
+
 int lcbi_gpu_binary_mag(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_settings,
                         const lcbi_lens_model* models, int32_t n_models, int64_t n, const lcbi_fs_point* points,
                         lcbi_fs_result* results, unsigned flags)
 {
-    Context* ctx = reinterpret_cast<Context*>(c);
+    return binary_mag_impl(reinterpret_cast<Context*>(c), settings, n_settings, models, n_models, n, points, results,
+                           nullptr, flags);
+}
+
+int lcbi_gpu_binary_mag_grad(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_settings,
+                             const lcbi_lens_model* models, int32_t n_models, int64_t n, const lcbi_fs_point* points,
+                             lcbi_fs_result* results, double* grads, unsigned flags)
+{
+    if (!grads) return LCBI_INVALID_ARGUMENT;
+    return binary_mag_impl(reinterpret_cast<Context*>(c), settings, n_settings, models, n_models, n, points, results,
+                           grads, flags);
+}
+
+} // extern "C"
+
+namespace lcbi {
+namespace {
+int binary_mag_impl(Context* ctx, const lcbi_fs_settings* settings, int32_t n_settings, const lcbi_lens_model* models,
+                    int32_t n_models, int64_t n, const lcbi_fs_point* points, lcbi_fs_result* results, double* grads,
+                    unsigned flags)
+{
     if (!ctx || n < 0 || !settings || n_settings <= 0) return LCBI_INVALID_ARGUMENT;
     if (n == 0) return LCBI_OK;
     if (!points || !results) return LCBI_INVALID_ARGUMENT;
@@ -424,7 +463,16 @@ int lcbi_gpu_binary_mag(lcbi_gpu_context* c, const lcbi_fs_settings* settings, i
             return LCBI_GPU_ERROR;
     }
     if (!ctx->ensure(ctx->fs_out, n * sizeof(FsOut))) return LCBI_GPU_ERROR;
-    if (!run_pipeline(ctx, plan, n)) return LCBI_GPU_ERROR;
+    double* dgrads = nullptr;
+    if (grads) {
+        if (dev) {
+            dgrads = grads;
+        } else {
+            if (!ctx->ensure(ctx->fs_grad, (size_t)n * 8 * sizeof(double))) return LCBI_GPU_ERROR;
+            dgrads = static_cast<double*>(ctx->fs_grad.ptr);
+        }
+    }
+    if (!run_pipeline(ctx, plan, n, dgrads)) return LCBI_GPU_ERROR;
     if (dev) {
         if (!ctx->check("results D2D", cudaMemcpyAsync(results, ctx->fs_out.ptr, n * sizeof(FsOut),
                                                        cudaMemcpyDeviceToDevice, ctx->stream)) ||
@@ -432,8 +480,15 @@ int lcbi_gpu_binary_mag(lcbi_gpu_context* c, const lcbi_fs_settings* settings, i
             return LCBI_GPU_ERROR;
         return LCBI_OK;
     }
+    if (grads && !ctx->check("gradients D2H", cudaMemcpyAsync(grads, dgrads, (size_t)n * 8 * sizeof(double),
+                                                               cudaMemcpyDeviceToHost, ctx->stream)))
+        return LCBI_GPU_ERROR;
     return finish_results(ctx, results, n);
 }
+} // namespace
+} // namespace lcbi
+
+extern "C" {
 
 int lcbi_gpu_binary_inverse_ray(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int64_t n, const double* s,
                                 const double* q, const double* y1, const double* y2, const double* rho, double* A,
@@ -516,6 +571,91 @@ int lcbi_gpu_light_curves(lcbi_gpu_context* c, const lcbi_fs_settings* settings,
         return LCBI_GPU_ERROR;
     ctx->launches += 1;
     if (!run_pipeline(ctx, plan, n_times)) return LCBI_GPU_ERROR;
+    std::vector<lcbi_fs_result> res(static_cast<size_t>(n_times));
+    const int rc = finish_results(ctx, res.data(), n_times);
+    if (rc != LCBI_OK) return rc;
+    for (long long i = 0; i < n_times; ++i) {
+        A[i] = res[i].magnification;
+        if (method) method[i] = res[i].method;
+        if (status) status[i] = res[i].status;
+    }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_models,
+                               const double* params, const int64_t* first, const int32_t* count, const double* times,
+                               int64_t n_times, double* A, double* dA, int32_t* method, int32_t* status)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !settings || n_models < 0 || n_times < 0) return LCBI_INVALID_ARGUMENT;
+    if (n_models == 0 || n_times == 0) return LCBI_OK;
+    if (!params || !first || !count || !times || !A) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    if (!check_settings(ctx, settings, 1)) return LCBI_UNSUPPORTED;
+    // One settings entry per distinct Gamma (the models' linear limb darkening).
+    std::vector<lcbi_fs_settings> sts;
+    std::vector<int> model_settings(static_cast<size_t>(n_models));
+    for (int m = 0; m < n_models; ++m) {
+        const double g = params[8 * m + 7];
+        int idx = -1;
+        for (size_t k = 0; k < sts.size(); ++k)
+            if (sts[k].limb_darkening_c == g) idx = static_cast<int>(k);
+        if (idx < 0) {
+            lcbi_fs_settings st = settings[0];
+            st.limb_darkening_c = g;
+            st.limb_darkening_d = 0.0;
+            idx = static_cast<int>(sts.size());
+            sts.push_back(st);
+        }
+        model_settings[m] = idx;
+    }
+    Plan plan;
+    add_settings(plan, sts.data(), static_cast<int>(sts.size()));
+    ModelTable mt{&plan};
+    std::vector<LcModel> lcm(static_cast<size_t>(n_models));
+    for (int m = 0; m < n_models; ++m) {
+        const double* p = params + 8 * m;
+        if (first[m] < 0 || count[m] < 0 || first[m] + count[m] > n_times) return LCBI_INVALID_ARGUMENT;
+        LcModel& L = lcm[m];
+        L.t0 = p[0];
+        L.tE = p[1];
+        L.u0 = p[2];
+        L.cos_alpha = std::cos(p[3]);
+        L.sin_alpha = std::sin(p[3]);
+        L.s = p[4];
+        L.q_core = p[5] != 0.0 ? 1.0 / p[5] : p[5];
+        L.rho = p[6];
+        L.first = first[m];
+        L.count = count[m];
+        L.settings = model_settings[m];
+        L.model = (p[6] != 0.0 && settings->finite_mode > 0) ? mt.get(L.s, L.q_core, settings->caustic_bins) : 0;
+        L.pad = 0;
+    }
+    if (!upload(ctx, ctx->fs_lc_models, lcm) || !ctx->ensure(ctx->fs_times, n_times * sizeof(double)) ||
+        !ctx->check("times H2D", cudaMemcpyAsync(ctx->fs_times.ptr, times, n_times * sizeof(double),
+                                                 cudaMemcpyHostToDevice, ctx->stream)) ||
+        !ctx->ensure(ctx->fs_items, n_times * sizeof(FsItem)) || !ctx->ensure(ctx->fs_out, n_times * sizeof(FsOut)) ||
+        !ctx->ensure(ctx->fs_grad, (size_t)n_times * 8 * sizeof(double)) ||
+        !ctx->ensure(ctx->fs_grad_lc, (size_t)n_times * 8 * sizeof(double)))
+        return LCBI_GPU_ERROR;
+    const LcModel* dm = static_cast<LcModel*>(ctx->fs_lc_models.ptr);
+    const double* dt = static_cast<double*>(ctx->fs_times.ptr);
+    if (!ctx->check("lc items", launch_lc_items(dm, n_models, dt, static_cast<FsItem*>(ctx->fs_items.ptr), n_times,
+                                                ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    double* pg = dA ? static_cast<double*>(ctx->fs_grad.ptr) : nullptr;
+    if (!run_pipeline(ctx, plan, n_times, pg)) return LCBI_GPU_ERROR;
+    if (dA) {
+        if (!ctx->check("gradient chain", launch_lc_grad_chain(dm, n_models, dt, pg,
+                                                               static_cast<double*>(ctx->fs_grad_lc.ptr), n_times,
+                                                               ctx->stream)) ||
+            !ctx->check("gradients D2H", cudaMemcpyAsync(dA, ctx->fs_grad_lc.ptr, (size_t)n_times * 8 * sizeof(double),
+                                                         cudaMemcpyDeviceToHost, ctx->stream)))
+            return LCBI_GPU_ERROR;
+        ctx->launches += 1;
+    }
     std::vector<lcbi_fs_result> res(static_cast<size_t>(n_times));
     const int rc = finish_results(ctx, res.data(), n_times);
     if (rc != LCBI_OK) return rc;

@@ -44,4 +44,42 @@ cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* t
     return cudaGetLastError();
 }
 
+// Chain rule from the point parameters (y1, y2, s, q_core, rho, c) to the
+// light-curve parameters (t0, tE, u0, alpha, s, q, rho, Gamma), with
+// q_core = 1 / q and Gamma = c.
+__global__ void lc_grad_chain_kernel(const LcModel* __restrict__ models, int n_models,
+                                     const double* __restrict__ times, const double* __restrict__ pg,
+                                     double* __restrict__ out, long long n_items)
+{
+    const int m = blockIdx.y;
+    if (m >= n_models) return;
+    const LcModel md = models[m];
+    const double inverse_tE = 1.0 / md.tE;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < md.count; i += gridDim.x * blockDim.x) {
+        const long long k = md.first + i;
+        if (k >= n_items) break;
+        const double tau = (times[k] - md.t0) * inverse_tE;
+        const double* g = pg + k * 8;
+        const double along = g[0] * md.cos_alpha + g[1] * md.sin_alpha;
+        double* o = out + k * 8;
+        o[0] = -along * inverse_tE;
+        o[1] = -along * tau * inverse_tE;
+        o[2] = -g[0] * md.sin_alpha + g[1] * md.cos_alpha;
+        o[3] = g[0] * (-tau * md.sin_alpha - md.u0 * md.cos_alpha) + g[1] * (tau * md.cos_alpha - md.u0 * md.sin_alpha);
+        o[4] = g[2];
+        o[5] = -g[3] * md.q_core * md.q_core;
+        o[6] = md.rho < 0.0 ? -g[4] : g[4];
+        o[7] = g[5];
+    }
+}
+
+cudaError_t launch_lc_grad_chain(const LcModel* models, int n_models, const double* times, const double* point_grads,
+                                 double* grads, long long n_items, cudaStream_t stream)
+{
+    if (n_models <= 0) return cudaSuccess;
+    dim3 grid(4, n_models);
+    lc_grad_chain_kernel<<<grid, 256, 0, stream>>>(models, n_models, times, point_grads, grads, n_items);
+    return cudaGetLastError();
+}
+
 } // namespace lcbi

@@ -32,7 +32,7 @@ struct Context {
     Buffer fs_settings, fs_models, fs_raw_offset, fs_phases, fs_items, fs_out, fs_raw, fs_branches, fs_ld;
     Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
     Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
-    Buffer fs_cycles, fs_tiles;
+    Buffer fs_cycles, fs_tiles, fs_grad_tiles, fs_grad, fs_grad_lc;
     bool trig_ready = false;
     unsigned long long epoch = 0;
     int fs_warps = 0;          // persistent warps the scratch areas are sized for
@@ -46,6 +46,7 @@ struct Context {
     // Second pass, one block of kBigWarps warps per point, for the points that
     // pass the first pass's cell budget or overflow its per-warp scratch.
     long long cell_budget = 1 << 19;
+    bool cell_budget_set = false;  // set by the caller; else small batches send every point to blocks
     int retry_blocks = 0;      // 0: one per SM
     int row_cap_big = 1 << 19;
     int queue_cap_big = 1 << 19;
@@ -55,6 +56,9 @@ struct Context {
     bool polar_tiles = true;
     long long tile_capacity = 1 << 20;
     int tile_blocks = 0;       // persistent flood blocks (0: occupancy x SMs)
+    // Adjoint: cells per source radius of the gradient lattice, flood blocks.
+    int grad_bins = 48;
+    int grad_blocks = 0;
     cudaStream_t own_stream = nullptr;  // the context's stream; `stream` may be a caller's
 
     // Optional per-stage kernel timing with CUDA events on the launch stream.
@@ -77,7 +81,7 @@ struct Context {
         for (Buffer* b : {&fs_settings, &fs_models, &fs_raw_offset, &fs_phases, &fs_items, &fs_out, &fs_raw,
                           &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
                           &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
-                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles})
+                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc})
             v.push_back(b);
         return v;
     }

@@ -102,6 +102,12 @@ cudaError_t launch_polar_tiles(const FsWork& w, void* area, long long capacity, 
 size_t tile_bytes(long long capacity, int max_items);
 int polar_tile_blocks_per_sm();
 size_t seed_candidate_bytes_per_warp(int cand_cap);
+// Adjoint: dA/d(y1, y2, s, q, rho, c), the value differentiated and the method
+// of every point of the work lists (8 doubles per point).
+cudaError_t launch_grad(const FsWork& w, void* area, long long capacity, int max_items, int flood_blocks,
+                        int grad_bins, int sm_count, double* grads, cudaStream_t stream);
+size_t grad_tile_bytes(long long capacity, int max_items);
+int grad_flood_blocks_per_sm();
 size_t cartesian_scratch_bytes(int row_cap, int seed_cap);
 size_t polar_scratch_bytes(int queue_cap, int hash_cap);
 
@@ -117,5 +123,9 @@ struct LcModel {
 };
 cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* times, FsItem* items,
                             long long n_items, cudaStream_t stream);
+// Per-epoch gradients of light curves, (t0, tE, u0, alpha, s, q, rho, Gamma),
+// from the per-point gradients of launch_grad; `rho_sign` per model.
+cudaError_t launch_lc_grad_chain(const LcModel* models, int n_models, const double* times, const double* point_grads,
+                                 double* grads, long long n_items, cudaStream_t stream);
 
 } // namespace lcbi

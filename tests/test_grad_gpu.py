@@ -1,0 +1,199 @@
+"""GPU tests of the adjoint (lcbi_gpu_binary_mag_grad, lcbi_gpu_light_curves_grad
+and the torch.autograd.Function over them).
+
+Bars: point source and hexadecapole gradients are exact derivatives of the
+forward's closed forms, so they match central finite differences of the
+forward (relative step 1e-6) to 1e-5.  Inverse-ray gradients are the exact
+gradients of a piecewise-linear approximation of the continuum magnification
+(reported beside them), so they match its finite differences to 2e-3 (median,
+scaled by the parameter's size; 1e-2 at the 75th percentile, the rest from
+kinks of the piecewise-linear approximation and lattice squares joining the
+visited set); that value agrees with the lattice forward to 2e-2,
+and the source-position gradients match finite differences of the converged
+lattice forward (nbin 200, steps of 0.05 rho) to 3e-2 (median).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _settings(mode=4, nbin=50, c=0.3, forced_ir=False):
+    import lcbinint_b200 as lb
+    st = lb.Options(nbin=nbin).fs_settings(lb.LimbDarkening.linear(c))
+    st.finite_mode = mode
+    if forced_ir:
+        st.kinji_threshold = 1e18
+        st.hex_threshold = 0.0
+        st.adaptive_hex_threshold = 0.0
+    return st
+
+
+def _run(points_rows, settings_list):
+    """rows: (s, q_core, y1, y2, rho, settings index) -> (results, grads (n, 8))."""
+    from lcbinint_b200 import _lib
+    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, PS_EXACT, PS_ON_DEVICE, LcbiStructs
+    rows = np.asarray(points_rows, dtype=np.float64)
+    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
+    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
+    pts["settings"] = rows[:, 5].astype(np.int32)
+    pts["flags"] = PS_EXACT | PS_ON_DEVICE
+    res = np.zeros(len(rows), dtype=FS_RESULT_DTYPE)
+    grads = np.zeros((len(rows), 8))
+    st = (LcbiStructs.FsSettings * len(settings_list))(*settings_list)
+    ctx = _lib.context(0)
+    rc = ctx._L.lcbi_gpu_binary_mag_grad(ctx.handle, st, len(settings_list), None, 0, len(rows), pts.ctypes.data,
+                                         res.ctypes.data, grads.ctypes.data, 0)
+    ctx.check(rc, "lcbi_gpu_binary_mag_grad")
+    return res, grads
+
+
+def _near_caustic(n, seed, rho_range=(2e-3, 2e-2), spread=3.0):
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(seed)
+    rows = []
+    while len(rows) < n:
+        s = float(np.exp(rng.uniform(np.log(0.6), np.log(1.6))))
+        q = float(np.exp(rng.uniform(np.log(1e-3), 0.0)))
+        rho = float(np.exp(rng.uniform(np.log(rho_range[0]), np.log(rho_range[1]))))
+        br, _, _ = Oracle().caustic_cache(s, q, 256)
+        pts = br.reshape(-1, 2)
+        p = pts[rng.integers(len(pts))] + rng.normal(0.0, spread * rho, 2)
+        rows.append([s, q, p[0], p[1], rho])
+    return np.array(rows)
+
+
+def _fd(rows, sidx, settings, k, h):
+    """Central differences of (A, slot 6) in point parameter k (0 y1, 1 y2, 2 s, 3 q, 4 rho)."""
+    col = {0: 2, 1: 3, 2: 0, 3: 1, 4: 4}[k]
+    up = rows.copy()
+    dn = rows.copy()
+    up[:, col] += h
+    dn[:, col] -= h
+    ru, gu = _run(np.column_stack([up, sidx]), settings)
+    rd, gd = _run(np.column_stack([dn, sidx]), settings)
+    return ru, rd, gu, gd
+
+
+def test_point_source_gradient_matches_finite_differences():
+    rows = _near_caustic(200, seed=1, spread=20.0)
+    st = [_settings(mode=0)]
+    sidx = np.zeros(len(rows))
+    res, g = _run(np.column_stack([rows, sidx]), st)
+    assert (res["method"] == 0).all()
+    A = res["magnification"]
+    ok = A < 200.0
+    for k in range(4):
+        col = {0: 2, 1: 3, 2: 0, 3: 1}[k]
+        h = 1e-6 * np.maximum(np.abs(rows[:, col]), 0.1)
+        up, dn = rows.copy(), rows.copy()
+        up[:, col] += h
+        dn[:, col] -= h
+        ru, _ = _run(np.column_stack([up, sidx]), st)
+        rd, _ = _run(np.column_stack([dn, sidx]), st)
+        fd = (ru["magnification"] - rd["magnification"]) / (2 * h)
+        scale = np.abs(fd) + A / np.maximum(np.abs(rows[:, col]), 0.1)
+        err = np.abs(g[:, k] - fd) / scale
+        assert np.nanmax(err[ok]) < 1e-5, (k, np.nanmax(err[ok]))
+    assert np.all(g[:, 4] == 0.0) and np.all(g[:, 5] == 0.0)
+
+
+def test_hexadecapole_gradient_matches_finite_differences():
+    rows = _near_caustic(300, seed=2, spread=6.0)
+    st = [_settings(mode=4, c=0.4), _settings(mode=4, c=0.4 + 1e-6), _settings(mode=4, c=0.4 - 1e-6)]
+    sidx = np.zeros(len(rows))
+    res, g = _run(np.column_stack([rows, sidx]), st)
+    hexm = res["method"] == 1
+    assert hexm.sum() > 30
+    A = res["magnification"]
+    for k in range(5):
+        col = {0: 2, 1: 3, 2: 0, 3: 1, 4: 4}[k]
+        h = 1e-6 * np.abs(rows[:, col]) if k >= 2 else np.full(len(rows), 1e-6)
+        ru, rd, _, _ = _fd(rows, sidx, st, k, h)
+        same = hexm & (ru["method"] == 1) & (rd["method"] == 1)
+        fd = (ru["magnification"] - rd["magnification"]) / (2 * h)
+        size = np.abs(rows[:, col]) if k >= 2 else rows[:, 4]
+        err = np.abs(g[:, k] - fd) * size / A
+        assert np.nanmax(err[same]) < 1e-5, (k, np.nanmax(err[same]))
+    ru, _ = _run(np.column_stack([rows, np.ones(len(rows))]), st)
+    rd, _ = _run(np.column_stack([rows, np.full(len(rows), 2.0)]), st)
+    same = hexm & (ru["method"] == 1) & (rd["method"] == 1)
+    fd = (ru["magnification"] - rd["magnification"]) / 2e-6
+    assert np.nanmax(np.abs(g[same, 5] - fd[same]) / A[same]) < 1e-5
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_inverse_ray_gradient_matches_its_continuum_value(mode):
+    rows = _near_caustic(24, seed=3 + mode, rho_range=(3e-3, 1e-2), spread=1.0)
+    c = 0.45
+    st = [_settings(mode=mode, nbin=50, c=c, forced_ir=True), _settings(mode=mode, nbin=50, c=c + 1e-4, forced_ir=True),
+          _settings(mode=mode, nbin=50, c=c - 1e-4, forced_ir=True)]
+    sidx = np.zeros(len(rows))
+    res, g = _run(np.column_stack([rows, sidx]), st)
+    assert (res["method"] == mode + 1).all() and (res["status"] == 0).all()
+    A = res["magnification"]
+    Ac = g[:, 6]
+    assert np.all(np.isfinite(g[:, :7]))
+    # the continuum value the gradient differentiates agrees with the lattice forward
+    assert np.max(np.abs(Ac / A - 1.0)) < 2e-2, np.max(np.abs(Ac / A - 1.0))
+    rho = rows[:, 4]
+    for k, h, size in ((0, 1e-4 * rho, rho), (1, 1e-4 * rho, rho), (2, 1e-6 * rows[:, 0], rows[:, 0]),
+                       (3, 1e-6 * rows[:, 1], rows[:, 1])):
+        _, _, gu, gd = _fd(rows, sidx, st, k, h)
+        fd = (gu[:, 6] - gd[:, 6]) / (2 * h)
+        err = np.abs(g[:, k] - fd) * size / Ac
+        # The approximation is piecewise smooth (kinks where a lattice vertex
+        # crosses a level), and a lattice cell that joins the visited set
+        # adds a step of one square, so some points see finite-difference
+        # error at any step; the bar is on the median and the 75th percentile.
+        assert np.median(err) < 2e-3 and np.percentile(err, 75) < 1e-2, \
+            (k, np.median(err), np.percentile(err, 75), np.max(err))
+    _, gu = _run(np.column_stack([rows, np.ones(len(rows))]), st)
+    _, gd = _run(np.column_stack([rows, np.full(len(rows), 2.0)]), st)
+    fd = (gu[:, 6] - gd[:, 6]) / 2e-4
+    err = np.abs(g[:, 5] - fd) / Ac
+    assert np.median(err) < 1e-3 and np.max(err) < 1e-2, (np.median(err), np.max(err))
+
+
+def test_inverse_ray_gradient_matches_converged_forward():
+    rows = _near_caustic(12, seed=9, rho_range=(5e-3, 1e-2), spread=0.8)
+    st = [_settings(mode=1, nbin=200, c=0.3, forced_ir=True)]
+    sidx = np.zeros(len(rows))
+    res, g = _run(np.column_stack([rows, sidx]), st)
+    A = res["magnification"]
+    rho = rows[:, 4]
+    # The lattice forward moves in steps of its cells, so its differences need
+    # steps of several cells; the bar is on the median over the points.
+    for k, h, size in ((0, 0.05 * rho, rho), (1, 0.05 * rho, rho)):
+        ru, rd, _, _ = _fd(rows, sidx, st, k, h)
+        fd = (ru["magnification"] - rd["magnification"]) / (2 * h)
+        err = np.abs(g[:, k] - fd) * size / A
+        assert np.median(err) < 3e-2, (k, np.median(err), np.max(err))
+
+
+def test_light_curve_autograd_matches_finite_differences():
+    import torch
+    from lcbinint_b200.autograd import light_curve_magnification, light_curves_with_grad
+    # Point-source and hexadecapole epochs: an event away from the caustic.
+    P = np.array([[0.1, 20.0, 0.3, 0.7, 1.3, 0.01, 1e-3, 0.4], [-0.2, 15.0, 0.25, 2.0, 0.8, 0.05, 2e-3, 0.2]])
+    T = np.linspace(-30.0, 30.0, 40)
+    A, dA, method, status = light_curves_with_grad(P, T)
+    assert (status == 0).all() and np.isin(method, [0, 1]).all()
+    for j in range(8):
+        h = 1e-6 * max(abs(P[0, j]), 1e-2)
+        up, dn = P.copy(), P.copy()
+        up[:, j] += h
+        dn[:, j] -= h
+        Au, _, mu, _ = light_curves_with_grad(up, T, with_grad=False)
+        Ad, _, md, _ = light_curves_with_grad(dn, T, with_grad=False)
+        same = (mu == method) & (md == method)
+        fd = (Au - Ad) / (2 * h)
+        err = np.abs(dA[..., j] - fd) * max(abs(P[0, j]), 1e-2) / A
+        assert np.max(err[same]) < 1e-5, (j, np.max(err[same]))
+    params = torch.tensor(P, requires_grad=True)
+    At = light_curve_magnification(params, torch.tensor(T))
+    assert np.array_equal(At.detach().numpy(), A)
+    At.sum().backward()
+    assert np.allclose(params.grad.numpy(), dA.sum(axis=1), rtol=1e-12, atol=0)

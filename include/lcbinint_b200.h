@@ -282,13 +282,13 @@ int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context *ctx, const lcbi_fs_settings *s
 /* Same types, field order, names and semantics as include/lcbinint/lcbinint.h,
  * so a program written against the reference's header links against this
  * library unchanged.  The magnification runs on the calling thread's current
- * CUDA device, through a context kept per host thread.  Built: static binary
- * lenses (q2 <= 0, no parallax, no xallarap, LCBI_ORBIT_STATIC) in both
+ * CUDA device, through a context kept per host thread.  Built: binary lenses
+ * (q2 <= 0, no parallax, no xallarap), static or with circular or Keplerian
+ * lens orbital motion (src/lcbinint/model/orbital_motion.cpp:69-206), in both
  * coordinate conventions, point and finite source, bit-identical to the
  * reference.  Parameter sets that need the rest (triple lenses, parallax,
- * xallarap, lens orbital motion) return LCBI_UNSUPPORTED, with the result
- * filled as the reference fills it for unsupported input (NaN
- * magnifications, the source position). */
+ * xallarap) return LCBI_UNSUPPORTED, with the result filled as the reference
+ * fills it for unsupported input (NaN magnifications, the source position). */
 #ifndef LCBININT_H
 typedef enum lcbi_orbital_motion_mode {
     LCBI_ORBIT_STATIC = 0,

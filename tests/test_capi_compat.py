@@ -155,6 +155,9 @@ def test_invalid_and_unsupported_input():
     p.piEN = 0.1  # annual parallax is not built
     assert L.lcbi_magnification(0.0, C.byref(p), C.byref(o), C.byref(r)) == 3
     p = L.lcbi_default_params()
+    p.q2 = 0.1  # triple lenses are not built
+    assert L.lcbi_magnification(0.0, C.byref(p), C.byref(o), C.byref(r)) == 3
+    p = L.lcbi_default_params()
     p.omega = 0.1  # unsupported in the reference too
     assert L.lcbi_magnification(0.0, C.byref(p), C.byref(o), C.byref(r)) == 3
     assert math.isnan(r.magnification)
@@ -191,6 +194,52 @@ def test_matches_compiled_reference_bit_for_bit(vbm, com, rho, mode):
         o.mode = mode
         o.source_bins = 30
         times = np.ascontiguousarray(np.linspace(p.t0 - 1.5 * p.tE, p.t0 + 1.5 * p.tE, 60))
+        a = (Result * len(times))()
+        b = (Result * len(times))()
+        ra = ours.lcbi_magnification_array(times.ctypes.data, len(times), C.byref(p), C.byref(o), a)
+        rb = ref.lcbi_magnification_array(times.ctypes.data, len(times), C.byref(p), C.byref(o), b)
+        assert ra == rb
+        fa, fb = _fields(a), _fields(b)
+        for f in fa:
+            x, y = fa[f], fb[f]
+            if x.dtype.kind == "f":
+                assert np.array_equal(np.isnan(x), np.isnan(y)), f
+                ok = ~np.isnan(x)
+                assert np.array_equal(x[ok].view(np.int64), y[ok].view(np.int64)), \
+                    (f, np.nanmax(np.abs(x / y - 1.0)))
+            else:
+                assert np.array_equal(x, y), f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,vbm,rho", [(1, 1, 0.0), (1, 0, 3e-3), (2, 1, 5e-3), (2, 0, 0.0)])
+def test_orbital_motion_matches_compiled_reference(mode, vbm, rho):
+    """Circular (1) and Keplerian (2) lens orbital motion through the C ABI,
+    over 200 days, bit for bit against the compiled reference."""
+    ours = _ours()
+    ref = _reference()
+    rng = np.random.default_rng(200 + 10 * mode + vbm)
+    for _ in range(2):
+        p = ours.lcbi_default_params()
+        o = ours.lcbi_default_options()
+        p.t0 = 0.0
+        p.tE = float(rng.uniform(15.0, 40.0))
+        p.umin = float(rng.uniform(-0.2, 0.2))
+        p.theta = float(rng.uniform(0.0, 2.0 * np.pi))
+        p.sep = float(np.exp(rng.uniform(np.log(0.6), np.log(1.6))))
+        p.q = float(np.exp(rng.uniform(np.log(1e-3), 0.0)))
+        p.rho = rho
+        p.limb_darkening_c = 0.4
+        p.orbital_motion_mode = mode
+        p.g1 = float(rng.uniform(-1.0, 1.0)) / 365.25
+        p.g2 = float(rng.uniform(-1.0, 1.0)) / 365.25
+        p.g3 = float(rng.uniform(0.0, 0.5)) / 365.25
+        if mode == 2:
+            p.lom_szs = float(rng.uniform(-0.5, 0.5))
+            p.lom_ar = float(rng.uniform(1.0, 2.0))
+        o.vbm_compatible = vbm
+        o.source_bins = 30
+        times = np.ascontiguousarray(np.linspace(-100.0, 100.0, 80))
         a = (Result * len(times))()
         b = (Result * len(times))()
         ra = ours.lcbi_magnification_array(times.ctypes.data, len(times), C.byref(p), C.byref(o), a)

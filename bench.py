@@ -2,7 +2,7 @@
 """Benchmark of the lcbinint B200 magnification path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload fs_batch|ps_batch|light_curve]
+                    [--workload fs_batch|ps_batch|light_curve|adjoint|orbital]
 
 Default workload (fs_batch): the uneven finite-source batch -- 4,096 light-curve
 points from 64 random binary-lens models (s log-U[0.3,3], q log-U[1e-5,1], rho
@@ -284,6 +284,73 @@ def cpu_adjoint_rate(P, T, n_procs, n_models):
     return n / wall / 17.0, n, wall
 
 
+def orbital_workload(seed=3, n_models=1024, n_epochs=2000):
+    """Config 5, its lens-orbital-motion half: models drawn as in config 3
+    (t0 U[-20, 20] d, tE U[10, 40] d), half of them on circular and half on
+    Keplerian orbits with ds/dt / s and dalpha/dt U[-1, 1] per year and the
+    line-of-sight term g3 U[0, 0.5] per year (Keplerian: lom_szs U[-0.5, 0.5],
+    lom_ar U[1, 2]); 2000 epochs spanning 200 days.  Returns the parameter
+    dictionaries, their orbital-motion modes, their limb-darkening
+    coefficients and the epochs."""
+    rng = np.random.default_rng(seed)
+    dicts, modes, gams = [], [], []
+    for m in range(n_models):
+        p = dict(t0=float(rng.uniform(-20.0, 20.0)), tE=float(rng.uniform(10.0, 40.0)),
+                 u0=float(rng.uniform(-0.2, 0.2)), alpha=float(rng.uniform(0.0, 2.0 * np.pi)),
+                 s=float(np.exp(rng.uniform(np.log(0.3), np.log(3.0)))), q=float(np.exp(rng.uniform(np.log(1e-5), 0.0))),
+                 rho=float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2)))),
+                 g1=float(rng.uniform(-1.0, 1.0)) / 365.25, g2=float(rng.uniform(-1.0, 1.0)) / 365.25,
+                 g3=float(rng.uniform(0.0, 0.5)) / 365.25)
+        mode = 1 if m % 2 == 0 else 2
+        if mode == 2:
+            p.update(lom_szs=float(rng.uniform(-0.5, 0.5)), lom_ar=float(rng.uniform(1.0, 2.0)))
+        dicts.append(p)
+        modes.append(mode)
+        gams.append(float(rng.uniform(0.0, 0.8)))
+    return dicts, modes, gams, np.linspace(-100.0, 100.0, n_epochs)
+
+
+def _ref_orbital_worker(args):
+    """One process: the reference's LightCurve (dictionary route) on a list of
+    (parameters, mode, Gamma, epochs) tasks."""
+    tasks, = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import import_reference_module
+    ref = import_reference_module()
+    modes = [ref.STATIC, ref.CIRCULAR, ref.KEPLER]
+    t = time.perf_counter()
+    n = 0
+    for p, mode, gam, times in tasks:
+        lc = ref.LightCurve(limb_darkening=ref.LimbDarkening.linear(gam), orbital_motion_mode=modes[mode])
+        lc(times, p)
+        n += len(times)
+    return time.perf_counter() - t, n
+
+
+def cpu_orbital_rate(dicts, modes, gams, times, n_procs, target_seconds):
+    """Magnifications/s of the reference on a bounded sample: runs of 25
+    consecutive epochs from random models, one process per core, sized to
+    about target_seconds (1.5-2 ms per epoch on one core: every epoch
+    re-samples the caustic of its own separation)."""
+    import multiprocessing as mp
+    rng = np.random.default_rng(13)
+    run = 25
+    per_epoch = 2.0e-3
+    n_runs = int(max(n_procs, target_seconds * n_procs / (per_epoch * run)))
+    tasks = []
+    for _ in range(n_runs):
+        m = int(rng.integers(len(dicts)))
+        e = int(rng.integers(len(times) - run))
+        tasks.append((dicts[m], modes[m], gams[m], times[e:e + run]))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n_procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_ref_orbital_worker, [(tasks[k::n_procs],) for k in range(n_procs)])
+        wall = time.perf_counter() - t0
+    n = sum(r[1] for r in res)
+    return n / wall, n, wall
+
+
 def _ref_ps_worker(args):
     s, q, y1, y2, reps = args
     sys.path.insert(0, str(ROOT))
@@ -343,6 +410,9 @@ def run_other_workload(args, world, rank, local_rank, ncores):
                   "parallelism": f"replicas x{world}"}
     if args.workload == "adjoint":
         run_adjoint(args, world, rank, local_rank, ncores, common)
+        return
+    if args.workload == "orbital":
+        run_orbital(args, world, rank, local_rank, ncores, common)
         return
     if args.impl == "reference":
         if rank != 0:
@@ -577,6 +647,100 @@ def run_adjoint(args, world, rank, local_rank, ncores, common):
         print(json.dumps(out))
 
 
+def run_orbital(args, world, rank, local_rank, ncores, common):
+    """Config 5, lens-orbital-motion half: 1024 models x 2000 epochs with
+    circular or Keplerian lens orbital motion through the batched C ABI
+    (lcbi_gpu_magnification_arrays, LensModel's route), host arrays in and
+    out.  The parallax half needs the reference's Earth ephemeris table,
+    which is missing, so parallax is not applied."""
+    dicts, modes, gams, times = orbital_workload(seed=3 + rank)
+    M, K = len(dicts), times.size
+    n = M * K
+    config = {"workload": "orbital: 1024 models x 2000 epochs over 200 days, half circular / half Keplerian lens "
+                          "orbital motion (g1, g2 U[-1,1]/yr, g3 U[0,0.5]/yr), config-3 model distribution, "
+                          "linear LD U[0,0.8], auto decision tree, nbin 50; parallax not applied (no ephemeris)",
+              "points": n, "l2": "not flushed (per-epoch caustic samples, 2.9 GB per chunk, exceed L2)",
+              "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rate, nn, wall = cpu_orbital_rate(dicts, modes, gams, times, ncores, max(4.0, args.cpu_seconds / 2))
+        out = dict(common, impl="reference", value=rate, n_gpus=args.gpus, ms_per_step=1e3 * n / rate,
+                   config=config,
+                   cpu_baseline={"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                                 "sample": f"{nn} epochs in runs of 25 from random models, {wall:.1f} s on "
+                                           f"{ncores} processes"},
+                   e2e={"value": rate, "unit": "magnifications/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(out))
+        return
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    import lcbinint_b200 as lb
+    from lcbinint_b200 import _lib, api
+    ctx = lb.context(local_rank)
+    L = ctx._L
+    cps = np.concatenate([api.binary_c_params([p], lb.LimbDarkening.linear(g), orbital_motion_mode=m)
+                          for p, m, g in zip(dicts, modes, gams)])
+    co = lb.Options().c_options()
+    first = (np.arange(M, dtype=np.int64) * K)
+    count = np.full(M, K, dtype=np.int32)
+    all_times = np.ascontiguousarray(np.tile(times, M))
+    res = np.zeros(n, dtype=_lib.RESULT_DTYPE)
+    status = np.zeros(M, dtype=np.int32)
+
+    def step():
+        rc = L.lcbi_gpu_magnification_arrays(ctx.handle, M, _lib.ptr(cps), _lib.ptr(co), _lib.ptr(first),
+                                             _lib.ptr(count), _lib.ptr(all_times), n, 0, _lib.ptr(res),
+                                             _lib.ptr(status))
+        ctx.check(rc, "lcbi_gpu_magnification_arrays")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    launches0 = ctx.launches
+    L.lcbi_gpu_set_timing(ctx.handle, 1)
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local_rank) as clocks:
+        wall = 0.0
+        for _ in range(args.steps):
+            torch.cuda.synchronize(dev)
+            t1 = time.perf_counter()
+            step()
+            wall += time.perf_counter() - t1
+    launches = (ctx.launches - launches0) // max(1, args.steps)
+    stage_ms = np.zeros(8)
+    stage_n = np.zeros(8, dtype=np.int64)
+    L.lcbi_gpu_stage_times(ctx.handle, _lib.ptr(stage_ms), _lib.ptr(stage_n), 8)
+    L.lcbi_gpu_set_timing(ctx.handle, 0)
+    (max_wall,), (n_all,) = reduce_over_ranks([wall], [n], world, dev)
+    value = n_all * args.steps / max_wall
+    names = ["caustics+ld", "decide", "seeds", "cartesian", "polar", "point_source"]
+    out = dict(common, value=value, n_gpus=world, ms_per_step=1e3 * max_wall / args.steps, config=config,
+               status_ok_sets=int((status == 0).sum()),
+               finite_source_evaluated=int(np.isfinite(res["finite_source_magnification"]).sum()),
+               stage_ms_per_step={names[i]: float(stage_ms[i]) / args.steps for i in range(6)},
+               timing="wall clock around the host-pointer call (host orbit geometry on the host cores, "
+                      "H2D, kernels, D2H); the device stages are CUDA-event timed",
+               e2e={"value": value, "unit": "magnifications/s", "h2d_bytes_per_step": int(cps.nbytes + all_times.nbytes),
+                    "d2h_bytes_per_step": int(res.nbytes + status.nbytes)},
+               gpu_launches=int(launches), clocks=clocks.summary())
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, nn, w = cpu_orbital_rate(dicts, modes, gams, times, ncores, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
+                               "sample": f"{nn} epochs in runs of 25 from random models, {w:.1f} s on {ncores} "
+                                         "processes"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 # --------------------------------------------------------------------------- main
 
 
@@ -604,7 +768,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch", "ps_batch", "light_curve", "adjoint"])
+    ap.add_argument("--workload", default="fs_batch", choices=["fs_batch", "ps_batch", "light_curve", "adjoint",
+                                                                   "orbital"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,

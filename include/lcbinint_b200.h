@@ -393,6 +393,29 @@ lcbi_status lcbi_magnification_array(const double *times, int count, const lcbi_
 const char *lcbi_status_string(lcbi_status status);
 #endif
 
+/* lcbi_magnification_array for many parameter sets in one batched GPU pass
+ * (no reference counterpart: the reference evaluates one set per call, one
+ * epoch at a time).  Set m covers times[first[m] .. first[m] + count[m]) and
+ * writes results[first[m] ...] and status[m] exactly as
+ * lcbi_magnification_array(times + first[m], count[m], params + m, options,
+ * results + first[m]) would.  Sets may differ in every parameter, lens orbital
+ * motion and limb darkening included; options (NULL: the defaults) is shared.
+ * Lens orbital motion gives every epoch its own separation, hence its own
+ * caustic sampling (1,400 quartics by default), as in the reference.
+ * With LCBI_ARRAYS_KEYWORD_ROUTE the source is turned into the orbit's frame
+ * as the Python module's keyword-argument light curves turn it
+ * (python/lcbinint_pybind.cpp:1985-2008: the trajectory point rotated back
+ * by alpha and forward by the orbit's angle) instead of as LensModel does
+ * (src/lcbinint/model/lens_model.cpp:172-190); the two differ in rounding
+ * only.  Returns LCBI_OK once every set has its status, else the error that
+ * stopped the batch (LCBI_INVALID_ARGUMENT for bad array arguments,
+ * LCBI_GPU_ERROR). */
+#define LCBI_ARRAYS_KEYWORD_ROUTE 1u
+int lcbi_gpu_magnification_arrays(lcbi_gpu_context *ctx, int32_t n_sets, const lcbi_params *params,
+                                  const lcbi_options *options, const int64_t *first, const int32_t *count,
+                                  const double *times, int64_t n_times, unsigned flags, lcbi_result *results,
+                                  int32_t *status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,53 @@ LCBI_UNSUPPORTED = 3
 LCBI_GPU_ERROR = 16
 DEVICE_POINTERS = 1
 
+# The reference's C ABI structs (include/lcbinint/lcbinint.h:46-116) as numpy
+# record types with C alignment, for arrays of parameter sets and results.
+_PARAMS_HEAD = ("t0", "tE", "umin", "q", "sep", "theta", "rho", "omega", "piEN", "piEE", "piEN_xa", "piEE_xa",
+                "ra_xa", "dec_xa", "period_xa", "ecc_xa", "peri_xa", "v_sep", "q2", "sep2", "ang", "ra", "dec",
+                "earth_axis", "tfix", "obs_lat", "obs_lon", "limb_darkening_c", "limb_darkening_d")
+_PARAMS_TAIL = ("g1", "g2", "g3", "lom_szs", "lom_ar", "xi_1", "xi_2", "omega_xa", "inc_xa", "phi_xa")
+PARAMS_DTYPE = np.dtype([(n, "f8") for n in _PARAMS_HEAD] + [("orbital_motion_mode", "i4")] +
+                        [(n, "f8") for n in _PARAMS_TAIL], align=True)
+OPTIONS_DTYPE = np.dtype([("parallax_mode", "i4"), ("orbit_pair", "i4"), ("center_of_mass", "i4"),
+                          ("caustic_bins", "i4"), ("source_bins", "i4"), ("mode", "i4"), ("vbm_compatible", "i4"),
+                          ("xallarap_param_type", "i4"), ("grid_ratio", "f8"), ("polar_source_bins", "i4"),
+                          ("polar_grid_ratio", "f8"), ("point_source_threshold", "f8"),
+                          ("hexadecapole_threshold", "f8"), ("adaptive_hex_threshold", "f8"),
+                          ("adaptive_source_bins", "i4"), ("max_source_bins", "i4"), ("finite_source_tol", "f8"),
+                          ("finite_source_reltol", "f8")], align=True)
+RESULT_DTYPE = np.dtype([("magnification", "f8"), ("point_source_magnification", "f8"),
+                         ("finite_source_magnification", "f8"), ("source_x", "f8"), ("source_y", "f8"),
+                         ("image_count", "i4"), ("finite_source_error_estimate", "f8"),
+                         ("finite_source_refinement_level", "i4"), ("finite_source_converged", "i4")], align=True)
+ARRAYS_KEYWORD_ROUTE = 1
+
+
+def default_params(n: int = 1) -> np.ndarray:
+    """lcbi_default_params (lcbinint.h:118) for n parameter sets."""
+    p = np.zeros(n, dtype=PARAMS_DTYPE)
+    p["tE"] = 1.0
+    p["q"] = 1.0
+    p["sep"] = 1.0
+    p["lom_ar"] = 1.0
+    return p
+
+
+def default_options() -> np.ndarray:
+    """lcbi_default_options (lcbinint.h:119), as a one-element array."""
+    o = np.zeros(1, dtype=OPTIONS_DTYPE)
+    o["orbit_pair"] = 23
+    o["caustic_bins"] = 1400
+    o["source_bins"] = 50
+    o["mode"] = 4
+    o["grid_ratio"] = 4.0
+    o["point_source_threshold"] = 20.0
+    o["hexadecapole_threshold"] = 3.0
+    o["adaptive_hex_threshold"] = 0.001
+    o["max_source_bins"] = 400
+    return o
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _vp = C.c_void_p
@@ -94,6 +141,9 @@ def _declare(L):
     L.lcbi_gpu_last_ray_counts.restype = C.c_int
     L.lcbi_gpu_binary_mag_noalloc.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_int64, _vp, _vp, _vp, _vp]
     L.lcbi_gpu_binary_mag_noalloc.restype = C.c_int
+    L.lcbi_gpu_magnification_arrays.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_uint, _vp,
+                                                 _vp]
+    L.lcbi_gpu_magnification_arrays.restype = C.c_int
 
 
 def exported_symbols() -> list[str]:

@@ -101,6 +101,9 @@ def _apply_param_type(o: "Options", name: str):
         raise ValueError("param_type must be 'vbm', 'lcbinint', 'original', or 'center_of_mass'")
 
 
+_XALLARAP_TYPE = {"": 0, "none": 0, "angular_velocity": 1, "orbital_elements": 2}
+
+
 class Options:
     """Computation options; defaults and aliases of lcbinint.Options (PYB:2985-3112)."""
 
@@ -213,6 +216,28 @@ class Options:
     @property
     def xallarap_param_type(self) -> str:
         return self._xallarap
+
+    def c_options(self) -> np.ndarray:
+        """The lcbi_options this Options stands for (PYB:2985-3037 on top of
+        public_default_options, PYB:213-220), as a one-element array."""
+        o = _lib.default_options()
+        o["center_of_mass"] = self.center_of_mass
+        o["vbm_compatible"] = self.vbm_compatible
+        o["mode"] = self._mode
+        o["xallarap_param_type"] = _XALLARAP_TYPE[self._xallarap]
+        o["source_bins"] = self.source_bins
+        o["caustic_bins"] = self.caustic_bins
+        o["grid_ratio"] = self.grid_ratio
+        o["polar_source_bins"] = self.polar_source_bins
+        o["polar_grid_ratio"] = self._polar_grid_ratio
+        o["point_source_threshold"] = self.point_source_threshold
+        o["hexadecapole_threshold"] = self.hexadecapole_threshold
+        o["adaptive_hex_threshold"] = self.adaptive_hex_threshold
+        o["adaptive_source_bins"] = self.adaptive_source_bins
+        o["max_source_bins"] = self.max_source_bins
+        o["finite_source_tol"] = self.finite_source_tol
+        o["finite_source_reltol"] = self.finite_source_reltol
+        return o
 
     def fs_settings(self, ld: LimbDarkening) -> LcbiStructs.FsSettings:
         """make_finite_source_settings (PYB:471-492)."""
@@ -329,14 +354,100 @@ STATIC = 0
 CIRCULAR = 1
 KEPLER = 2
 
+# Parameter-dictionary keys and defaults (PyBinaryParams, PYB:103-134).
+_BINARY_PARAM_DEFAULTS = dict(t0=0.0, tE=1.0, u0=0.0, alpha=0.0, s=1.0, q=1.0, q2=0.0, sep2=0.0, ang=0.0, rho=0.0,
+                              piEN=0.0, piEE=0.0, g1=0.0, g2=0.0, g3=0.0, lom_szs=0.0, lom_ar=1.0, u0_2=0.0,
+                              t0_2=0.0, flux_ratio=0.0, xi_1=0.0, xi_2=0.0, omega_xa=0.0, inc_xa=0.0, phi_xa=0.0,
+                              piEN_xa=0.0, piEE_xa=0.0, period_xa=0.0, ecc_xa=0.0, peri_xa=0.0)
+
+
+def binary_c_params(params_list, limb_darkening: LimbDarkening = None, event: EventCoordinates = None,
+                    orbital_motion_mode: int = STATIC, parallax: bool = False,
+                    terrestrial_parallax: bool = False) -> np.ndarray:
+    """lcbi_params of single-source binary-lens parameter dictionaries, as
+    make_c_params_for_single_source builds them (PYB:2721-2748, with
+    make_binary_params PYB:338-401): the parallax components count only with
+    parallax, the observatory only with terrestrial parallax."""
+    ld = limb_darkening or LimbDarkening()
+    ev = event or EventCoordinates()
+    out = _lib.default_params(len(params_list))
+    for i, d in enumerate(params_list):
+        p = dict(_BINARY_PARAM_DEFAULTS)
+        p.update(d)
+        r = out[i]
+        r["t0"], r["tE"], r["umin"], r["theta"] = p["t0"], p["tE"], p["u0"], p["alpha"]
+        r["sep"], r["q"], r["rho"] = p["s"], p["q"], p["rho"]
+        r["limb_darkening_c"], r["limb_darkening_d"] = ld.c, ld.d
+        r["ra"], r["dec"], r["tfix"] = ev.ra, ev.dec, ev.tfix
+        if terrestrial_parallax:
+            r["obs_lat"], r["obs_lon"] = ev.obs_lat, ev.obs_lon
+        if parallax:
+            r["piEN"], r["piEE"] = p["piEN"], p["piEE"]
+        r["g1"], r["g2"], r["g3"] = p["g1"], p["g2"], p["g3"]
+        r["orbital_motion_mode"] = int(orbital_motion_mode)
+        r["lom_szs"], r["lom_ar"] = p["lom_szs"], p["lom_ar"]
+        for k in ("xi_1", "xi_2", "omega_xa", "inc_xa", "phi_xa", "piEN_xa", "piEE_xa", "period_xa", "ecc_xa",
+                  "peri_xa"):
+            r[k] = p[k]
+    return out
+
+
+def magnification_arrays(times_list, c_params: np.ndarray, options: Options = None, *, keyword_route: bool = False,
+                         device: int = 0):
+    """lcbi_magnification_array for many parameter sets in one batched GPU
+    pass (lcbi_gpu_magnification_arrays).  c_params is an array of
+    PARAMS_DTYPE records (binary_c_params builds them from dictionaries).
+    Returns (results, status): per set an array of RESULT_DTYPE records and
+    the status lcbi_magnification_array would have returned."""
+    opt = options or Options()
+    c_params = np.ascontiguousarray(c_params, dtype=_lib.PARAMS_DTYPE)
+    nm = len(c_params)
+    counts = np.array([len(t) for t in times_list], dtype=np.int32)
+    first = np.zeros(nm, dtype=np.int64)
+    if nm > 1:
+        first[1:] = np.cumsum(counts[:-1])
+    times = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64).ravel() for t in times_list])
+                                 if nm else np.zeros(0))
+    res = np.zeros(times.size, dtype=_lib.RESULT_DTYPE)
+    status = np.zeros(nm, dtype=np.int32)
+    if nm == 0:
+        return [], status
+    co = opt.c_options()
+    ctx = context(device)
+    rc = ctx._L.lcbi_gpu_magnification_arrays(ctx.handle, nm, _lib.ptr(c_params), _lib.ptr(co), _lib.ptr(first),
+                                              _lib.ptr(counts), _lib.ptr(times), times.size,
+                                              _lib.ARRAYS_KEYWORD_ROUTE if keyword_route else 0, _lib.ptr(res),
+                                              _lib.ptr(status))
+    ctx.check(rc, "lcbi_gpu_magnification_arrays")
+    return np.split(res, np.cumsum(counts)[:-1]), status
+
+
+def _raise_for_c_status(status):
+    # direct_dynamic_fill_values / evaluate_binary_light_curve_numpy (PYB:1074-1083, 1160-1171)
+    for st in np.asarray(status).ravel():
+        if st == _lib.LCBI_UNSUPPORTED:
+            raise RuntimeError("unsupported")
+        if st == _lib.LCBI_INVALID_ARGUMENT:
+            raise ValueError("invalid argument")
+        if st != _lib.LCBI_OK:
+            raise RuntimeError("numerical error")
+
 
 class LightCurve:
     """lcbinint.LightCurve (PYB:3114-3406): a reusable light-curve callable.
 
-    The static binary lens in VBM coordinates (the reference's direct fast
-    path, PYB:1087-1174) and binary sources (PYB:2331-2354) run on the GPU.
-    Orbital motion, parallax and the original/centre-of-mass conventions are
-    not implemented and raise NotImplementedError."""
+    Routes as the reference does.  The static binary lens in VBM coordinates
+    takes the direct fast path (PYB:1087-1174, lcbi_gpu_light_curves).  Lens
+    orbital motion (circular or Keplerian) and the original / centre-of-mass
+    conventions take LensModel's path when the parameters come as a
+    dictionary (PYB:2325-2358 -> lens_model.cpp) and the dynamic path when
+    they come as keywords (PYB:1364-1385, 1958-2060); both run through
+    lcbi_gpu_magnification_arrays.  Binary sources blend two single-source
+    curves (PYB:2331-2354).  Parallax needs the reference's Earth ephemeris
+    and triple lenses are outside this implementation: both raise
+    NotImplementedError."""
+
+    _KEYWORDS = ("t0", "tE", "u0", "alpha", "s", "q", "rho", "piEN", "piEE", "g1", "g2", "g3", "lom_szs", "lom_ar")
 
     def __init__(self, *, lens: str = "binary_lens", source: str = "single", event: EventCoordinates = None,
                  options: Options = None, limb_darkening: LimbDarkening = None, orbital_motion_mode: int = STATIC,
@@ -351,36 +462,54 @@ class LightCurve:
             source = "binary"
         else:
             raise ValueError("source must be 'single' or 'binary'")
+        if parallax or terrestrial_parallax:
+            raise NotImplementedError("parallax needs the reference's Earth ephemeris table, which is not available")
         self.lens = "binary_lens"
         self.source = source
         self.event = event or EventCoordinates()
         self.options = options or Options()
         self.limb_darkening = limb_darkening or LimbDarkening()
-        self.orbital_motion_mode = orbital_motion_mode
+        self.orbital_motion_mode = int(orbital_motion_mode)
+        if self.orbital_motion_mode not in (STATIC, CIRCULAR, KEPLER):
+            raise ValueError("orbital_motion_mode must be STATIC, CIRCULAR or KEPLER")
         self.parallax = parallax
         self.terrestrial_parallax = terrestrial_parallax
 
-    def _check_supported(self, p):
-        if self.orbital_motion_mode != STATIC or self.parallax or self.terrestrial_parallax:
-            raise NotImplementedError("orbital motion and parallax are not implemented on the GPU path")
-        if not (self.options.vbm_compatible and not self.options.center_of_mass):
-            raise NotImplementedError("only the 'vbm' coordinate convention is implemented")
-        for k in ("piEN", "piEE", "xi_1", "xi_2", "piEN_xa", "piEE_xa"):
-            if p.get(k, 0.0) != 0.0:
-                raise NotImplementedError(f"{k} != 0 is not implemented on the GPU path")
+    def _direct(self, p=None) -> bool:
+        # can_use_direct_static_binary (PYB:494-503); for dictionaries also
+        # evaluate_binary_light_curve_numpy's test (PYB:1105-1118).
+        o = self.options
+        if not (self.orbital_motion_mode == STATIC and o.vbm_compatible and not o.center_of_mass):
+            return False
+        if p is not None:
+            return all(p.get(k, 0.0) == 0.0 for k in ("xi_1", "xi_2", "piEN_xa", "piEE_xa"))
+        return True
 
-    def _single(self, times, p):
-        self._check_supported(p)
-        (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
-        _raise_for_status(st)
-        return A
+    def _single(self, times, p, keyword_route=False):
+        if self._direct(None if keyword_route else p):
+            (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
+            _raise_for_status(st)
+            return A
+        cp = binary_c_params([p], self.limb_darkening, self.event, self.orbital_motion_mode)
+        (res,), status = magnification_arrays([times], cp, self.options, keyword_route=keyword_route)
+        _raise_for_c_status(status)
+        return res["magnification"].copy()
 
     def __call__(self, times, params=None, **kw):
         times = np.ascontiguousarray(times, dtype=np.float64)
         if times.ndim != 1:
             raise ValueError("times must be one-dimensional")
-        p = dict(params) if params is not None else {}
-        p.update(kw)
+        if params is not None:
+            if kw:
+                raise TypeError("pass the parameters either as a dictionary or as keywords")
+            p = dict(params)
+            keyword_route = False
+        else:
+            unknown = set(kw) - set(self._KEYWORDS)
+            if unknown:
+                raise TypeError(f"unexpected keyword arguments: {sorted(unknown)}")
+            p = dict(kw)
+            keyword_route = True
         if self.source == "binary":
             p2 = dict(p)
             p2["u0"] = p.get("u0_2", 0.0)
@@ -390,7 +519,7 @@ class LightCurve:
             fr = p.get("flux_ratio", 0.0)
             inv = 1.0 / (1.0 + fr)
             return (v1 + fr * v2) * inv
-        return self._single(times, p)
+        return self._single(times, p, keyword_route)
 
     light_curve = __call__
 
@@ -405,7 +534,8 @@ class LightCurve:
         times = np.ascontiguousarray(times, dtype=np.float64)
         p = dict(params) if params is not None else {}
         p.update(kw)
-        self._check_supported(p)
+        if not self._direct(p):
+            raise NotImplementedError("info() is implemented for the static binary lens in VBM coordinates")
         (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
         _raise_for_status(st)
         return LightCurveInfo(times=list(times), magnifications=list(A), finite_source_methods=list(m),

@@ -11,9 +11,13 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <limits>
+#include <thread>
 #include <vector>
+
+#include "lcbi_internal.h"
 
 namespace {
 
@@ -208,6 +212,179 @@ void set_unevaluated(lcbi_result& r, double sx, double sy)
     r.finite_source_converged = 1;
 }
 
+// What LensModel::magnification (lens_model.cpp:83-236) settles for one
+// parameter set before the magnifier call.
+struct SetInfo {
+    int status = LCBI_OK;     // LCBI_OK: the first n_valid epochs go to the device
+    long long n_valid = 0;
+    double bad_x = 0.0, bad_y = 0.0;  // trajectory source of the first epoch without a finite orbit
+    bool write_first = false;  // results[0] is written as unevaluated at (first_x, first_y)
+    double first_x = 0.0, first_y = 0.0;
+    int settings = 0;
+};
+
+lcbi_fs_settings fs_settings_of(const lcbi_options& o, double c, double d)
+{
+    lcbi_fs_settings fs{};
+    fs.source_bins = o.source_bins;
+    fs.caustic_bins = o.caustic_bins;
+    fs.grid_ratio = o.grid_ratio;
+    fs.polar_source_bins = o.polar_source_bins;
+    fs.polar_grid_ratio = o.polar_grid_ratio;
+    fs.finite_mode = o.mode;
+    fs.kinji_threshold = o.point_source_threshold;
+    fs.hex_threshold = o.hexadecapole_threshold;
+    fs.adaptive_hex_threshold = o.adaptive_hex_threshold;
+    fs.limb_darkening_c = c;
+    fs.limb_darkening_d = d;
+    fs.adaptive_source_bins = o.adaptive_source_bins;
+    fs.max_source_bins = o.max_source_bins;
+    fs.finite_source_tol = o.finite_source_tol;
+    fs.finite_source_reltol = o.finite_source_reltol;
+    return fs;
+}
+
+// A cheap placeholder for an epoch that is not evaluated (a point source at
+// the centre of an equal-mass binary); its result is never read.
+void placeholder(lcbi_fs_point& pt)
+{
+    pt.s = 1.0;
+    pt.q = 1.0;
+    pt.y1 = 0.0;
+    pt.y2 = 0.0;
+    pt.rho = 0.0;
+    pt.point_source_magnification = 0.0;
+    pt.settings = 0;
+    pt.model = 0;
+    pt.flags = 0;
+    pt.reserved = 0;
+}
+
+// The static trajectory (lens_model.cpp:90-99), the orbit at each epoch
+// (:104-118) and the source in the orbit's frame (:162-190) for one set;
+// epochs that are not evaluated get placeholders.  The first epoch whose orbit
+// is not finite ends the set, as in the reference.
+void prepare_set(const lcbi_params& p, const lcbi_options& o, bool keyword_route, const double* times, long long n,
+                 double* sx, double* sy, lcbi_fs_point* pts, SetInfo& info)
+{
+    for (long long i = 0; i < n; ++i) placeholder(pts[i]);
+    if (n == 0) return;
+    if (!params_valid(p)) {
+        info.status = LCBI_INVALID_ARGUMENT;
+        return;
+    }
+    const bool vbm = o.vbm_compatible != 0;
+    const bool has_xallarap = o.xallarap_param_type != LCBI_XALLARAP_NONE &&
+                              (o.xallarap_param_type == LCBI_XALLARAP_ANGULAR_VELOCITY
+                                   ? (p.xi_1 != 0.0 || p.xi_2 != 0.0)
+                                   : (p.piEN_xa != 0.0 || p.piEE_xa != 0.0));
+    if (p.piEN != 0.0 || p.piEE != 0.0 || has_xallarap || p.q2 > 0.0) {
+        // Parallax, xallarap and triple lenses are not built here: the first
+        // epoch is reported as unsupported.
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        info.status = LCBI_UNSUPPORTED;
+        info.write_first = true;
+        info.first_x = nan;
+        info.first_y = nan;
+        return;
+    }
+    const double cos_t = std::cos(p.theta);
+    const double sin_t = std::sin(p.theta);
+    const bool static_orbit = p.orbital_motion_mode == LCBI_ORBIT_STATIC;
+    const double beta = p.umin;
+    const double eff_q = (vbm && p.q != 0.0) ? 1.0 / p.q : p.q;
+    const double rho = std::abs(p.rho);
+    long long n_valid = n;
+    for (long long i = 0; i < n; ++i) {
+        const double tn = (times[i] - p.t0) / p.tE;
+        double x, y;
+        if (vbm) {
+            x = tn * cos_t - beta * sin_t;
+            y = tn * sin_t + beta * cos_t;
+        } else {
+            x = beta * sin_t + tn * cos_t;
+            y = beta * cos_t - tn * sin_t;
+        }
+        const Orbit orb = static_orbit ? Orbit{p.sep, p.theta} : orbit_at(p, times[i]);
+        if (!std::isfinite(orb.separation) || !std::isfinite(orb.angle)) {
+            n_valid = i;
+            info.bad_x = x;
+            info.bad_y = y;
+            break;
+        }
+        if (!static_orbit) {
+            if (vbm) {
+                // LensModel rotates (tau, beta) directly; the keyword route
+                // first takes them back out of the trajectory point.
+                double tau = tn, b = beta;
+                if (keyword_route) {
+                    tau = x * cos_t + y * sin_t;
+                    b = -x * sin_t + y * cos_t;
+                }
+                const double nx = tau * std::cos(orb.angle) - b * std::sin(orb.angle);
+                const double ny = b * std::cos(orb.angle) + tau * std::sin(orb.angle);
+                x = nx;
+                y = ny;
+            } else {
+                // rotate_source_to_orbital_frame (orbital_motion.cpp:201-206).
+                const double c = std::cos(orb.angle - p.theta);
+                const double s = std::sin(orb.angle - p.theta);
+                const double rx = x * c + y * s;
+                const double ry = y * c - x * s;
+                x = rx;
+                y = ry;
+            }
+        }
+        sx[i] = x;
+        sy[i] = y;
+        lcbi_fs_point& pt = pts[i];
+        pt.s = orb.separation;
+        pt.q = eff_q;
+        pt.y1 = vbm ? x : x - wide_binary_offset(orb.separation, p, o);
+        pt.y2 = y;
+        pt.rho = rho;
+        pt.settings = info.settings;
+    }
+    if (n_valid == 0) {
+        info.status = LCBI_NUMERICAL_ERROR;
+        info.write_first = true;
+        info.first_x = info.bad_x;
+        info.first_y = info.bad_y;
+        return;
+    }
+    if (unsupported_dynamic(p, o)) {
+        for (long long i = 0; i < n_valid; ++i) placeholder(pts[i]);
+        info.status = LCBI_UNSUPPORTED;
+        info.write_first = true;
+        info.first_x = sx[0];
+        info.first_y = sy[0];
+        return;
+    }
+    for (long long i = n_valid; i < n; ++i) placeholder(pts[i]);
+    info.n_valid = n_valid;
+}
+
+// Runs fn(m) for every set, on several host threads when the batch is large
+// (each set writes only its own epochs).
+template <typename F>
+void parallel_sets(int n_sets, long long n_times, F fn)
+{
+    unsigned hw = std::thread::hardware_concurrency();
+    int threads = static_cast<int>(hw == 0 ? 1 : (hw > 32 ? 32 : hw));
+    if (threads > n_sets) threads = n_sets;
+    if (n_times < (1 << 16) || threads <= 1) {
+        for (int m = 0; m < n_sets; ++m) fn(m);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&]() {
+            for (int m = next.fetch_add(1); m < n_sets; m = next.fetch_add(1)) fn(m);
+        });
+    for (auto& th : pool) th.join();
+}
+
 } // namespace
 
 extern "C" {
@@ -249,159 +426,90 @@ lcbi_status lcbi_magnification_array(const double* times, int count, const lcbi_
     if (count < 0) return LCBI_INVALID_ARGUMENT;
     if (count == 0) return LCBI_OK;
     if (times == nullptr || params == nullptr || results == nullptr) return LCBI_INVALID_ARGUMENT;
-    const lcbi_params p = *params;
-    if (!params_valid(p)) return LCBI_INVALID_ARGUMENT;
-    // from_c_options (lens_parameters.cpp:59-85): no options means the defaults.
-    const lcbi_options o = options ? *options : lcbi_default_options();
-    const bool vbm = o.vbm_compatible != 0;
-    const size_t n = static_cast<size_t>(count);
-
-    const bool has_xallarap = o.xallarap_param_type != LCBI_XALLARAP_NONE &&
-                              (o.xallarap_param_type == LCBI_XALLARAP_ANGULAR_VELOCITY
-                                   ? (p.xi_1 != 0.0 || p.xi_2 != 0.0)
-                                   : (p.piEN_xa != 0.0 || p.piEE_xa != 0.0));
-    if (p.piEN != 0.0 || p.piEE != 0.0 || has_xallarap || p.q2 > 0.0) {
-        // Parallax, xallarap and triple lenses are not built here: report the
-        // first epoch as unsupported.
-        const double nan = std::numeric_limits<double>::quiet_NaN();
-        set_unevaluated(results[0], nan, nan);
-        return LCBI_UNSUPPORTED;
-    }
-
-    // Static trajectory (lens_model.cpp:90-99), the orbit at each epoch
-    // (:113-115) and the source in the orbit's frame (:172-190).  The first
-    // epoch whose orbit is not finite ends the array, as in the reference.
-    const double cos_t = std::cos(p.theta);
-    const double sin_t = std::sin(p.theta);
-    const bool static_orbit = p.orbital_motion_mode == LCBI_ORBIT_STATIC;
-    std::vector<double> sx(n), sy(n), mx(n), s_arr(n), q_arr(n);
-    const double beta = p.umin;
-    const double eff_q = (vbm && p.q != 0.0) ? 1.0 / p.q : p.q;
-    size_t n_valid = n;
-    double bad_x = 0.0, bad_y = 0.0;
-    for (size_t i = 0; i < n; ++i) {
-        const double tn = (times[i] - p.t0) / p.tE;
-        double x, y;
-        if (vbm) {
-            x = tn * cos_t - beta * sin_t;
-            y = tn * sin_t + beta * cos_t;
-        } else {
-            x = beta * sin_t + tn * cos_t;
-            y = beta * cos_t - tn * sin_t;
-        }
-        const Orbit orb = static_orbit ? Orbit{p.sep, p.theta} : orbit_at(p, times[i]);
-        if (!std::isfinite(orb.separation) || !std::isfinite(orb.angle)) {
-            n_valid = i;
-            bad_x = x;
-            bad_y = y;
-            break;
-        }
-        if (!static_orbit) {
-            if (vbm) {
-                const double nx = tn * std::cos(orb.angle) - beta * std::sin(orb.angle);
-                const double ny = beta * std::cos(orb.angle) + tn * std::sin(orb.angle);
-                x = nx;
-                y = ny;
-            } else {
-                // rotate_source_to_orbital_frame (orbital_motion.cpp:201-206).
-                const double c = std::cos(orb.angle - p.theta);
-                const double s = std::sin(orb.angle - p.theta);
-                const double rx = x * c + y * s;
-                const double ry = y * c - x * s;
-                x = rx;
-                y = ry;
-            }
-        }
-        sx[i] = x;
-        sy[i] = y;
-        mx[i] = vbm ? x : x - wide_binary_offset(orb.separation, p, o);
-        s_arr[i] = orb.separation;
-        q_arr[i] = eff_q;
-    }
-    if (n_valid == 0) {
-        set_unevaluated(results[0], bad_x, bad_y);
-        return LCBI_NUMERICAL_ERROR;
-    }
-    if (unsupported_dynamic(p, o)) {
-        set_unevaluated(results[0], sx[0], sy[0]);
-        return LCBI_UNSUPPORTED;
-    }
-    const int count_valid = static_cast<int>(n_valid);
     lcbi_gpu_context* ctx = thread_context();
     if (!ctx) return static_cast<lcbi_status>(LCBI_GPU_ERROR);
-    std::vector<double> A(n), A_ps(n), err(n, 0.0);
-    std::vector<int32_t> nimg(n), st(n, LCBI_OK), conv(n, 1);
+    const int64_t first = 0;
+    const int32_t n = count;
+    int32_t status = LCBI_OK;
+    const int rc = lcbi_gpu_magnification_arrays(ctx, 1, params, options, &first, &n, times, count, 0, results, &status);
+    return static_cast<lcbi_status>(rc != LCBI_OK ? rc : status);
+}
+
+int lcbi_gpu_magnification_arrays(lcbi_gpu_context* ctx, int32_t n_sets, const lcbi_params* params,
+                                  const lcbi_options* options, const int64_t* first, const int32_t* count,
+                                  const double* times, int64_t n_times, unsigned flags, lcbi_result* results,
+                                  int32_t* status)
+{
+    if (!ctx || n_sets < 0 || n_times < 0) return LCBI_INVALID_ARGUMENT;
+    if (n_sets == 0) return LCBI_OK;
+    if (!params || !first || !count || !status || (n_times > 0 && (!times || !results))) return LCBI_INVALID_ARGUMENT;
+    for (int m = 0; m < n_sets; ++m)
+        if (first[m] < 0 || count[m] < 0 || first[m] + count[m] > n_times) return LCBI_INVALID_ARGUMENT;
+    // from_c_options (lens_parameters.cpp:59-85): no options means the defaults.
+    const lcbi_options o = options ? *options : lcbi_default_options();
+    const bool keyword_route = (flags & LCBI_ARRAYS_KEYWORD_ROUTE) != 0;
+
+    // One settings entry per distinct limb darkening.
+    std::vector<lcbi_fs_settings> sts;
+    std::vector<SetInfo> info(static_cast<size_t>(n_sets));
+    for (int m = 0; m < n_sets; ++m) {
+        const double c = params[m].limb_darkening_c, d = params[m].limb_darkening_d;
+        int idx = -1;
+        for (size_t k = 0; k < sts.size() && idx < 0; ++k)
+            if (sts[k].limb_darkening_c == c && sts[k].limb_darkening_d == d) idx = static_cast<int>(k);
+        if (idx < 0) {
+            idx = static_cast<int>(sts.size());
+            sts.push_back(fs_settings_of(o, c, d));
+        }
+        info[m].settings = idx;
+    }
+
+    const size_t n = static_cast<size_t>(n_times);
+    std::vector<double> sx(n), sy(n), a_ps(n);
+    std::vector<int32_t> nimg(n);
+    std::vector<lcbi_fs_point> pts(n);
+    std::vector<lcbi_fs_result> res(n);
+    parallel_sets(n_sets, n_times, [&](int m) {
+        prepare_set(params[m], o, keyword_route, times + first[m], count[m], sx.data() + first[m],
+                    sy.data() + first[m], pts.data() + first[m], info[m]);
+    });
+    if (n_times > 0) {
+        const int rc = lcbi::binary_mag_images(ctx, sts.data(), static_cast<int>(sts.size()), pts.data(), n_times,
+                                               res.data(), a_ps.data(), nimg.data());
+        if (rc != LCBI_OK) return rc;
+    }
     const double nan = std::numeric_limits<double>::quiet_NaN();
-    if (p.rho == 0.0) {
-        // supports_binary_point_source (lens_model.cpp:43-46): binary_mag0.
-        const int rc = lcbi_gpu_binary_mag0(ctx, count_valid, s_arr.data(), q_arr.data(), mx.data(), sy.data(), A.data(),
-                                            nimg.data(), nullptr, 0);
-        if (rc != LCBI_OK) return static_cast<lcbi_status>(rc);
-        A_ps = A;
-    } else {
-        // binary_images seeds and point-source value, then the finite-source
-        // decision tree (lens_model.cpp:209-226).
-        int rc = lcbi_gpu_binary_images_mag(ctx, count_valid, s_arr.data(), q_arr.data(), mx.data(), sy.data(),
-                                            A_ps.data(), nimg.data(), 0);
-        if (rc != LCBI_OK) return static_cast<lcbi_status>(rc);
-        lcbi_fs_settings fs{};
-        fs.source_bins = o.source_bins;
-        fs.caustic_bins = o.caustic_bins;
-        fs.grid_ratio = o.grid_ratio;
-        fs.polar_source_bins = o.polar_source_bins;
-        fs.polar_grid_ratio = o.polar_grid_ratio;
-        fs.finite_mode = o.mode;
-        fs.kinji_threshold = o.point_source_threshold;
-        fs.hex_threshold = o.hexadecapole_threshold;
-        fs.adaptive_hex_threshold = o.adaptive_hex_threshold;
-        fs.limb_darkening_c = p.limb_darkening_c;
-        fs.limb_darkening_d = p.limb_darkening_d;
-        fs.adaptive_source_bins = o.adaptive_source_bins;
-        fs.max_source_bins = o.max_source_bins;
-        fs.finite_source_tol = o.finite_source_tol;
-        fs.finite_source_reltol = o.finite_source_reltol;
-        std::vector<lcbi_fs_point> pts(n);
-        std::vector<lcbi_fs_result> res(n);
-        const double rho = std::abs(p.rho);
-        for (size_t i = 0; i < n; ++i) {
-            lcbi_fs_point& pt = pts[i];
-            pt.s = s_arr[i];
-            pt.q = eff_q;
-            pt.y1 = mx[i];
-            pt.y2 = sy[i];
-            pt.rho = rho;
-            pt.point_source_magnification = A_ps[i];
-            pt.settings = 0;
-            pt.model = 0;
-            pt.flags = LCBI_FS_PS_EXACT | LCBI_FS_SEED_HINTS;
-            pt.reserved = 0;
-        }
-        rc = lcbi_gpu_binary_mag(ctx, &fs, 1, nullptr, 0, count_valid, pts.data(), res.data(), 0);
-        if (rc != LCBI_OK) return static_cast<lcbi_status>(rc);
-        for (size_t i = 0; i < n; ++i) {
-            A[i] = res[i].magnification;
-            err[i] = res[i].error_estimate;
-            conv[i] = res[i].converged;
+    for (int m = 0; m < n_sets; ++m) {
+        const SetInfo& in = info[m];
+        lcbi_result* r = results + first[m];
+        status[m] = in.status;
+        if (in.write_first) set_unevaluated(r[0], in.first_x, in.first_y);
+        if (in.status != LCBI_OK) continue;
+        const long long k0 = first[m];
+        const double rho = params[m].rho;
+        for (long long i = 0; i < in.n_valid; ++i) {
+            const lcbi_fs_result& f = res[k0 + i];
             // A device limit (status 17-19) leaves no magnification.
-            if (res[i].status != LCBI_OK && res[i].status != LCBI_NUMERICAL_ERROR) A[i] = nan;
+            const double A = (f.status != LCBI_OK && f.status != LCBI_NUMERICAL_ERROR) ? nan : f.magnification;
+            lcbi_result& ri = r[i];
+            ri.magnification = A;
+            ri.point_source_magnification = a_ps[k0 + i];
+            ri.finite_source_magnification = rho == 0.0 ? nan : A;
+            ri.source_x = sx[k0 + i];
+            ri.source_y = sy[k0 + i];
+            ri.image_count = nimg[k0 + i];
+            ri.finite_source_error_estimate = f.error_estimate;
+            ri.finite_source_refinement_level = 0;
+            ri.finite_source_converged = f.converged ? 1 : 0;
+            if (!std::isfinite(A)) {
+                status[m] = LCBI_NUMERICAL_ERROR;
+                break;
+            }
         }
-    }
-    for (size_t i = 0; i < n_valid; ++i) {
-        lcbi_result& r = results[i];
-        r.magnification = A[i];
-        r.point_source_magnification = A_ps[i];
-        r.finite_source_magnification = p.rho == 0.0 ? nan : A[i];
-        r.source_x = sx[i];
-        r.source_y = sy[i];
-        r.image_count = nimg[i];
-        r.finite_source_error_estimate = err[i];
-        r.finite_source_refinement_level = 0;
-        r.finite_source_converged = conv[i] ? 1 : 0;
-        if (!std::isfinite(r.magnification)) return LCBI_NUMERICAL_ERROR;
-    }
-    if (n_valid < n) {
-        set_unevaluated(results[n_valid], bad_x, bad_y);
-        return LCBI_NUMERICAL_ERROR;
+        if (status[m] == LCBI_OK && in.n_valid < count[m]) {
+            set_unevaluated(r[in.n_valid], in.bad_x, in.bad_y);
+            status[m] = LCBI_NUMERICAL_ERROR;
+        }
     }
     return LCBI_OK;
 }

@@ -5,6 +5,7 @@
 #include "../../include/lcbinint_b200.h"
 #include "lcbi_context.h"
 #include "lcbi_fs_kernels.h"
+#include "lcbi_internal.h"
 #include "lcbi_kernels.h"
 
 #include <cmath>
@@ -148,6 +149,34 @@ struct ModelTable {
         const auto key = std::make_tuple(bs, bq, bins);
         auto it = index.find(key);
         if (it != index.end()) return it->second;
+        const int id = add(s, q, bins);
+        index[key] = id;
+        return id;
+    }
+
+    // As get, but keyed only on the previous call's key: runs of points with
+    // the same (s, q, bins) share one model and any other point gets its own.
+    // Equal keys sample equal caustics, so a repeat costs only its sampling;
+    // this keeps the table linear in time when every point has its own
+    // separation (lens orbital motion).
+    int get_sequential(double s, double q, int caustic_bins)
+    {
+        const int bins = caustic_bins > 32 ? caustic_bins : 32;
+        uint64_t bs, bq;
+        std::memcpy(&bs, &s, 8);
+        std::memcpy(&bq, &q, 8);
+        const auto key = std::make_tuple(bs, bq, bins);
+        if (last_id >= 0 && key == last_key) return last_id;
+        last_key = key;
+        last_id = add(s, q, bins);
+        return last_id;
+    }
+
+    std::tuple<uint64_t, uint64_t, int> last_key{};
+    int last_id = -1;
+
+    int add(double s, double q, int bins)
+    {
         auto po = phase_offset.find(bins);
         int off;
         if (po == phase_offset.end()) {
@@ -172,7 +201,6 @@ struct ModelTable {
         if (bins > plan->max_bins) plan->max_bins = bins;
         const int id = static_cast<int>(plan->models.size());
         plan->models.push_back(m);
-        index[key] = id;
         return id;
     }
 };
@@ -295,9 +323,11 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = n
         w.retry_polar = w.retry_cart + kChunk;
         w.cand_cap = ctx->cand_cap;
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
-        // A batch too small to fill the GPU with one warp per point (a single
-        // light curve, say) runs every inverse-ray point on a whole block.
-        w.cell_budget = (!ctx->cell_budget_set && cn <= 4 * ctx->sm_count) ? 1 : ctx->cell_budget;
+        // Too few inverse-ray points to fill the GPU with one warp per point (a
+        // single light curve, say, or a large batch that is mostly point
+        // sources) run every point on a whole block.
+        w.cell_budget = ctx->cell_budget;
+        w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
         if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
         cudaEvent_t ev;
         ctx->stage_begin(1, &ev);
@@ -666,6 +696,68 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* sett
     }
     return LCBI_OK;
 }
+
+} // extern "C"
+
+namespace lcbi {
+
+int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int n_settings,
+                      const lcbi_fs_point* points, long long n, lcbi_fs_result* results, double* a_ps,
+                      int32_t* image_count)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0 || !settings || n_settings <= 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!points || !results || !a_ps || !image_count) return LCBI_INVALID_ARGUMENT;
+    for (long long i = 0; i < n; ++i)
+        if (points[i].settings < 0 || points[i].settings >= n_settings) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    if (!check_settings(ctx, settings, n_settings)) return LCBI_UNSUPPORTED;
+    if (!ctx->ensure(ctx->fs_all_out, n * sizeof(FsOut)) || !ctx->ensure(ctx->fs_all_aps, n * sizeof(double)) ||
+        !ctx->ensure(ctx->fs_all_nimg, n * sizeof(int)))
+        return LCBI_GPU_ERROR;
+    FsOut* all_out = static_cast<FsOut*>(ctx->fs_all_out.ptr);
+    double* all_aps = static_cast<double*>(ctx->fs_all_aps.ptr);
+    int* all_nimg = static_cast<int*>(ctx->fs_all_nimg.ptr);
+    std::vector<FsItem> items;
+    for (long long e0 = 0; e0 < n; e0 += kChunk) {
+        const long long cn = (n - e0) < kChunk ? (n - e0) : kChunk;
+        Plan plan;
+        add_settings(plan, settings, n_settings);
+        ModelTable mt{&plan};
+        items.resize(static_cast<size_t>(cn));
+        std::memcpy(items.data(), points + e0, cn * sizeof(FsItem));
+        for (auto& it : items) {
+            const lcbi_fs_settings& st = settings[it.settings];
+            it.a_ps = 0.0;
+            it.flags = kItemPsExact | kItemSeedHints;
+            it.model = (it.rho > 0.0 && st.finite_mode > 0) ? mt.get_sequential(it.s, it.q, st.caustic_bins) : 0;
+        }
+        if (!upload(ctx, ctx->fs_items, items) || !ctx->ensure(ctx->fs_out, cn * sizeof(FsOut))) return LCBI_GPU_ERROR;
+        if (!ctx->check("images", launch_item_images(static_cast<FsItem*>(ctx->fs_items.ptr), cn, all_aps + e0,
+                                                     all_nimg + e0, ctx->sm_count, ctx->stream)))
+            return LCBI_GPU_ERROR;
+        ctx->launches += 1;
+        if (!run_pipeline(ctx, plan, cn)) return LCBI_GPU_ERROR;
+        if (!ctx->check("results D2D", cudaMemcpyAsync(all_out + e0, ctx->fs_out.ptr, cn * sizeof(FsOut),
+                                                       cudaMemcpyDeviceToDevice, ctx->stream)))
+            return LCBI_GPU_ERROR;
+    }
+    if (!ctx->check("results D2H", cudaMemcpyAsync(results, all_out, n * sizeof(lcbi_fs_result),
+                                                   cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->check("a_ps D2H", cudaMemcpyAsync(a_ps, all_aps, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                                ctx->stream)) ||
+        !ctx->check("images D2H", cudaMemcpyAsync(image_count, all_nimg, n * sizeof(int32_t),
+                                                  cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+} // namespace lcbi
+
+extern "C" {
 
 int lcbi_gpu_last_item_cycles(lcbi_gpu_context* c, int64_t n, int64_t* cycles)
 {

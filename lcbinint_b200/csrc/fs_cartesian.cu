@@ -563,7 +563,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         Ctx C;
         C.rays = 0;
         C.evals = 0;
-        C.budget = (W == 1 && !w.retry_pass) ? w.cell_budget : 0;
+        C.budget = (W == 1 && !w.retry_pass) ? (n <= w.few_points ? 1 : w.cell_budget) : 0;
         if (ns > 0 && rho > 0.0) {
             C.m = make_mapper(item.s, item.q);
             C.src = P2{item.x, item.y};

@@ -44,6 +44,49 @@ cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* t
     return cudaGetLastError();
 }
 
+// Point-source value and image count of each item, written into the item as
+// the decision's a_ps.  A finite source takes them from binary_images
+// (point_source_magnifier.cpp:723-778), whose images also seed the inverse
+// ray, as LensModel forms its finite-source call (lens_model.cpp:209-226); a
+// point source (rho == 0) from binary_mag0 (lens_model.cpp:43-46).
+__global__ void __launch_bounds__(128) item_images_kernel(FsItem* __restrict__ items, long long n,
+                                                         double* __restrict__ a_ps, int* __restrict__ nimg)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double s = items[i].s, q = items[i].q, x = items[i].x, y = items[i].y;
+        double a = 0.0;
+        int cnt = 0;
+        if (items[i].rho > 0.0) {
+            if (s != 0.0 && q > 0.0) {
+                const BinaryGeom g = make_geom(s, q, x, y);
+                dc pos[5];
+                double res[5], det[5];
+                cnt = image_candidates(g, pos, res, det);
+                for (int k = 0; k < cnt; ++k) a += 1.0 / fabs(det[k]);
+            }
+        } else {
+            const PsResult r = point_source(s, q, x, y);
+            a = r.magnification;
+            cnt = r.image_count;
+        }
+        items[i].a_ps = a;
+        a_ps[i] = a;
+        nimg[i] = cnt;
+    }
+}
+
+cudaError_t launch_item_images(FsItem* items, long long n, double* a_ps, int* nimg, int sm_count, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const int threads = 128;
+    long long blocks = (n + threads - 1) / threads;
+    const long long cap = (long long)sm_count * 16;
+    if (blocks > cap) blocks = cap;
+    item_images_kernel<<<(unsigned)blocks, threads, 0, stream>>>(items, n, a_ps, nimg);
+    return cudaGetLastError();
+}
+
 // Chain rule from the point parameters (y1, y2, s, q_core, rho, c) to the
 // light-curve parameters (t0, tE, u0, alpha, s, q, rho, Gamma), with
 // q_core = 1 / q and Gamma = c.

@@ -356,7 +356,8 @@ __device__ void polar_body(const FsWork& w, unsigned long long epoch, PolarList 
                         }
                     }
                     rays += (unsigned long long)(R - L + 1);
-                    if (W == 1 && !w.retry_pass && rays > (unsigned long long)w.cell_budget) {
+                    if (W == 1 && !w.retry_pass &&
+                        rays > (unsigned long long)(n <= w.few_points ? 1 : w.cell_budget)) {
                         over_budget = true;
                         break;
                     }

@@ -33,6 +33,7 @@ struct Context {
     Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
     Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
     Buffer fs_cycles, fs_tiles, fs_grad_tiles, fs_grad, fs_grad_lc;
+    Buffer fs_all_out, fs_all_aps, fs_all_nimg;  // whole-batch results of binary_mag_images
     bool trig_ready = false;
     unsigned long long epoch = 0;
     int fs_warps = 0;          // persistent warps the scratch areas are sized for
@@ -81,7 +82,8 @@ struct Context {
         for (Buffer* b : {&fs_settings, &fs_models, &fs_raw_offset, &fs_phases, &fs_items, &fs_out, &fs_raw,
                           &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
                           &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
-                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc})
+                          &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc,
+                          &fs_all_out, &fs_all_aps, &fs_all_nimg})
             v.push_back(b);
         return v;
     }

@@ -83,6 +83,9 @@ struct FsWork {
     // is handed to the second pass, which runs each point on a block of
     // kBigWarps warps.
     long long cell_budget;
+    // First pass only: when a list holds at most this many points (0: never),
+    // the budget is one cell, so every point of the list runs on a block.
+    int few_points;
 };
 
 constexpr int kBigWarps = 8;
@@ -123,6 +126,9 @@ struct LcModel {
 };
 cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* times, FsItem* items,
                             long long n_items, cudaStream_t stream);
+// a_ps and image count per item from binary_images (rho > 0) or binary_mag0
+// (rho == 0), written into the items and into a_ps[n], nimg[n].
+cudaError_t launch_item_images(FsItem* items, long long n, double* a_ps, int* nimg, int sm_count, cudaStream_t stream);
 // Per-epoch gradients of light curves, (t0, tE, u0, alpha, s, q, rho, Gamma),
 // from the per-point gradients of launch_grad; `rho_sign` per model.
 cudaError_t launch_lc_grad_chain(const LcModel* models, int n_models, const double* times, const double* point_grads,

@@ -109,6 +109,21 @@ def test_struct_layout_matches_reference_header(tmp_path):
     assert int(sizes[5]) == C.sizeof(Result)
 
 
+def test_record_dtypes_match_the_structs():
+    """The numpy records lcbinint_b200 passes to lcbi_gpu_magnification_arrays
+    have the structs' sizes and field offsets."""
+    from lcbinint_b200 import _lib
+    for dt, st in ((_lib.PARAMS_DTYPE, Params), (_lib.OPTIONS_DTYPE, Options), (_lib.RESULT_DTYPE, Result)):
+        assert dt.itemsize == C.sizeof(st)
+        for name, _ in st._fields_:
+            assert dt.fields[name][1] == getattr(st, name).offset, name
+    d = _lib.default_params(1)[0]
+    assert (d["tE"], d["q"], d["sep"], d["lom_ar"], d["orbital_motion_mode"]) == (1.0, 1.0, 1.0, 1.0, 0)
+    o = _lib.default_options()[0]
+    assert (o["caustic_bins"], o["source_bins"], o["mode"], o["orbit_pair"], o["max_source_bins"]) == \
+        (1400, 50, 4, 23, 400)
+
+
 def test_defaults_and_status_strings():
     L = _ours()
     p = L.lcbi_default_params()

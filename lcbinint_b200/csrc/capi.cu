@@ -53,6 +53,7 @@ Context::~Context()
     for (Buffer* b : all_buffers()) {
         if (b->ptr) cudaFree(b->ptr);
     }
+    if (pinned) cudaFreeHost(pinned);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (auto& p : pending) {
         cudaEventDestroy(p.second.first);

@@ -175,6 +175,15 @@ struct ModelTable {
     std::tuple<uint64_t, uint64_t, int> last_key{};
     int last_id = -1;
 
+    // Starts a new pass: later models get branch offsets from 0 in a fresh
+    // table of samples, and no key is shared with earlier models.
+    void restart_pass()
+    {
+        index.clear();
+        last_id = -1;
+        raw_total = 0;
+    }
+
     int add(double s, double q, int bins)
     {
         auto po = phase_offset.find(bins);
@@ -234,9 +243,130 @@ bool upload(Context* ctx, Buffer& b, const std::vector<T>& v)
                                                 ctx->stream));
 }
 
-// Runs the pipeline on device-resident items (ctx->fs_items) and writes device
-// results to ctx->fs_out.  Everything is asynchronous on ctx->stream.
-bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = nullptr)
+size_t cart_bytes_of(const Context* c) { return (cartesian_scratch_bytes(c->row_cap, c->seed_cap) + 255) & ~size_t(255); }
+size_t polar_bytes_of(const Context* c) { return (polar_scratch_bytes(c->queue_cap, c->hash_cap) + 255) & ~size_t(255); }
+
+// The parts of a work description every stage shares; callers set the points,
+// results, caustic tables, work lists and counters.
+FsWork common_work(Context* ctx)
+{
+    FsWork w{};
+    w.settings = static_cast<const FsSettingsDev*>(ctx->fs_settings.ptr);
+    w.ld_tables = static_cast<const double*>(ctx->fs_ld.ptr);
+    w.trig = trig_of(ctx);
+    w.seeds = static_cast<P2*>(ctx->fs_seeds.ptr);
+    w.seed_cap = ctx->seed_cap;
+    w.scratch = static_cast<char*>(ctx->fs_scratch.ptr);
+    w.scratch_per_warp = static_cast<long long>(cart_bytes_of(ctx));
+    w.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar.ptr);
+    w.scratch_polar_per_warp = static_cast<long long>(polar_bytes_of(ctx));
+    w.row_cap = ctx->row_cap;
+    w.queue_cap = ctx->queue_cap;
+    w.hash_cap = ctx->hash_cap;
+    w.retry_pass = 0;
+    w.cand_cap = ctx->cand_cap;
+    // Too few inverse-ray points to fill the GPU with one warp per point (a
+    // single light curve, say, or a large batch that is mostly point
+    // sources) run every point on a whole block.
+    w.cell_budget = ctx->cell_budget;
+    w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
+    return w;
+}
+
+void set_lists(FsWork& w, int* counters, int* lists, int* retry, long long cap_cart, long long cap_retry)
+{
+    w.ir_count = counters;
+    w.next_item = counters + 8;
+    w.ir_cart = lists;
+    w.ir_polar = lists + cap_cart;
+    w.retry_cart = retry;
+    w.retry_polar = retry + cap_retry;
+}
+
+// The decision of every point of w (work lists and counters reset first).
+bool stage_decide(Context* ctx, const FsWork& w)
+{
+    if (!ctx->check("counters", cudaMemsetAsync(w.ir_count, 0, 64 * sizeof(int), ctx->stream))) return false;
+    cudaEvent_t ev;
+    ctx->stage_begin(1, &ev);
+    if (!ctx->check("decide", launch_decide(w, ctx->sm_count, ctx->stream))) return false;
+    ctx->stage_end(1, ev);
+    return true;
+}
+
+// Seeds of every inverse-ray point of w's work lists (at most max_points).
+bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
+{
+    const int warps = ctx->fs_warps < max_points ? ctx->fs_warps : max_points;
+    if (warps <= 0) return true;
+    // Candidate keys and probes share one allocation: all warps' keys, then all probes.
+    const size_t per = seed_candidate_bytes_per_warp(ctx->cand_cap);
+    const size_t key_bytes = per * 8 / (8 + 16);
+    char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
+    cudaEvent_t ev;
+    ctx->stage_begin(2, &ev);
+    if (!ctx->check("seeds", launch_seeds(w, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
+                                          reinterpret_cast<P2*>(cb + key_bytes * ctx->fs_warps), warps)))
+        return false;
+    ctx->stage_end(2, ev);
+    return true;
+}
+
+// Inverse ray of every point of w's work lists: a first pass on warps (the
+// polar points on tiles), then a second on blocks for the points that passed
+// the cell budget or outgrew the first pass's scratch.  max_points bounds the
+// lists' lengths.
+bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
+{
+    if (max_points <= 0) return true;
+    const size_t cart_bytes = cart_bytes_of(ctx);
+    const size_t pol_bytes = polar_bytes_of(ctx);
+    if (++ctx->epoch >= 0xfff0ull) {
+        ctx->big_ready = false;
+        if (!ensure_big_scratch(ctx)) return false;
+        if (!ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart_bytes * ctx->fs_warps,
+                                                         ctx->stream)) ||
+            !ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff,
+                                                         pol_bytes * ctx->fs_warps, ctx->stream)))
+            return false;
+        ctx->epoch = 1;
+    }
+    const int warps = ctx->fs_warps < max_points ? ctx->fs_warps : max_points;
+    cudaEvent_t ev;
+    ctx->stage_begin(3, &ev);
+    if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
+    ctx->stage_end(3, ev);
+    ctx->stage_begin(4, &ev);
+    if (ctx->polar_tiles) {
+        if (!ctx->check("polar", launch_polar_tiles(w, ctx->fs_tiles.ptr, ctx->tile_capacity, max_points,
+                                                    ctx->tile_blocks, ctx->stream)))
+            return false;
+    } else if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) {
+        return false;
+    }
+    ctx->stage_end(4, ev);
+    FsWork r = w;
+    r.retry_pass = 1;
+    r.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
+    r.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
+    r.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar_big.ptr);
+    r.scratch_polar_per_warp = static_cast<long long>(polar_bytes_big(ctx));
+    r.row_cap = ctx->row_cap_big;
+    r.queue_cap = ctx->queue_cap_big;
+    r.hash_cap = ctx->hash_cap_big;
+    ctx->stage_begin(3, &ev);
+    if (!ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
+    ctx->stage_end(3, ev);
+    ctx->stage_begin(4, &ev);
+    if (!ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
+    ctx->stage_end(4, ev);
+    ctx->launches += 8;
+    return true;
+}
+
+// Everything before the caustic sampling: constant tables, the settings and
+// limb-darkening tables, and the per-context scratch.
+bool prepare_tables(Context* ctx, const Plan& plan)
 {
     // Candidate lists of the caustic-branch seed probes hold one entry per sampled point.
     if (4 * plan.max_bins > ctx->cand_cap) {
@@ -244,40 +374,53 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = n
         ctx->fs_warps = 0;  // re-size the per-warp areas
     }
     if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx)) return false;
-    const int nset = static_cast<int>(plan.settings.size());
-    const int nmod = static_cast<int>(plan.models.size());
     const int nld = static_cast<int>(plan.ld_coeffs.size());
     if (!upload(ctx, ctx->fs_settings, plan.settings) || !upload(ctx, ctx->fs_models, plan.models) ||
         !upload(ctx, ctx->fs_raw_offset, plan.raw_offset) || !upload(ctx, ctx->fs_phases, plan.phases) ||
-        !upload(ctx, ctx->fs_ld_coeffs, plan.ld_coeffs))
-        return false;
-    long long raw_total = 0;
-    for (const auto& m : plan.models) raw_total += 4ll * m.bins;
-    if (!ctx->ensure(ctx->fs_raw, (raw_total + 1) * sizeof(P2)) ||
-        !ctx->ensure(ctx->fs_branches, (raw_total + 1) * sizeof(P2)) ||
+        !upload(ctx, ctx->fs_ld_coeffs, plan.ld_coeffs) ||
         !ctx->ensure(ctx->fs_ld, (size_t)(nld + 1) * (kLdTable + 1) * sizeof(double)) ||
-        !ctx->ensure(ctx->fs_rays, (size_t)(n + 1) * sizeof(unsigned long long)) ||
-        (ctx->item_cycles && !ctx->ensure(ctx->fs_cycles, (size_t)(n + 1) * sizeof(long long))) ||
-        !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
-        !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
-        !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)) ||
-        !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)) ||
-        !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, kChunk)))
+        !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)))
         return false;
     if (ctx->tile_blocks == 0) ctx->tile_blocks = polar_tile_blocks_per_sm() * ctx->sm_count;
-    (void)nset;
-    cudaEvent_t t0;
-    ctx->stage_begin(0, &t0);
     if (!ctx->check("ld tables", launch_ld_tables(static_cast<double2*>(ctx->fs_ld_coeffs.ptr), nld,
                                                   static_cast<double*>(ctx->fs_ld.ptr), ctx->stream)))
         return false;
     ctx->launches += 1;
+    return true;
+}
+
+// Per-point ray counts (and cycles) of n points, zeroed.
+bool prepare_counts(Context* ctx, long long n)
+{
+    if (!ctx->ensure(ctx->fs_rays, (size_t)(n + 1) * sizeof(unsigned long long)) ||
+        (ctx->item_cycles && !ctx->ensure(ctx->fs_cycles, (size_t)(n + 1) * sizeof(long long))))
+        return false;
     if (!ctx->check("rays init", cudaMemsetAsync(ctx->fs_rays.ptr, 0, (size_t)n * sizeof(unsigned long long),
                                                  ctx->stream)))
         return false;
     if (ctx->item_cycles &&
         !ctx->check("cycles init", cudaMemsetAsync(ctx->fs_cycles.ptr, 0, (size_t)n * sizeof(long long), ctx->stream)))
         return false;
+    return true;
+}
+
+// Runs the pipeline on device-resident items (ctx->fs_items) and writes device
+// results to ctx->fs_out.  Everything is asynchronous on ctx->stream.
+bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = nullptr)
+{
+    if (!prepare_tables(ctx, plan) || !prepare_counts(ctx, n)) return false;
+    const int nmod = static_cast<int>(plan.models.size());
+    long long raw_total = 0;
+    for (const auto& m : plan.models) raw_total += 4ll * m.bins;
+    if (!ctx->ensure(ctx->fs_raw, (raw_total + 1) * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_branches, (raw_total + 1) * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, kChunk)))
+        return false;
+    cudaEvent_t t0;
+    ctx->stage_begin(0, &t0);
     if (nmod > 0) {
         if (!ctx->check("caustics", launch_caustics(static_cast<CausticModel*>(ctx->fs_models.ptr), nmod, plan.max_bins,
                                                     static_cast<double2*>(ctx->fs_phases.ptr),
@@ -288,102 +431,21 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = n
         ctx->launches += 2;
     }
     ctx->stage_end(0, t0);
-    const size_t cart_bytes = (cartesian_scratch_bytes(ctx->row_cap, ctx->seed_cap) + 255) & ~size_t(255);
-    const size_t pol_bytes = (polar_scratch_bytes(ctx->queue_cap, ctx->hash_cap) + 255) & ~size_t(255);
     for (long long c0 = 0; c0 < n; c0 += kChunk) {
         const int cn = static_cast<int>((n - c0) < kChunk ? (n - c0) : kChunk);
-        FsWork w{};
+        FsWork w = common_work(ctx);
         w.items = static_cast<const FsItem*>(ctx->fs_items.ptr) + c0;
-        w.settings = static_cast<const FsSettingsDev*>(ctx->fs_settings.ptr);
         w.models = static_cast<const CausticModel*>(ctx->fs_models.ptr);
         w.raw_offset = static_cast<const long long*>(ctx->fs_raw_offset.ptr);
         w.raw = static_cast<const P2*>(ctx->fs_raw.ptr);
         w.branches = static_cast<const P2*>(ctx->fs_branches.ptr);
-        w.ld_tables = static_cast<const double*>(ctx->fs_ld.ptr);
-        w.trig = trig_of(ctx);
         w.out = static_cast<FsOut*>(ctx->fs_out.ptr) + c0;
         w.n_items = cn;
-        int* counters = static_cast<int*>(ctx->fs_counters.ptr);
-        w.ir_count = counters;
-        w.next_item = counters + 8;
-        w.ir_cart = static_cast<int*>(ctx->fs_ir.ptr);
-        w.ir_polar = w.ir_cart + kChunk;
-        w.seeds = static_cast<P2*>(ctx->fs_seeds.ptr);
-        w.seed_cap = ctx->seed_cap;
-        w.scratch = static_cast<char*>(ctx->fs_scratch.ptr);
-        w.scratch_per_warp = static_cast<long long>(cart_bytes);
-        w.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar.ptr);
-        w.scratch_polar_per_warp = static_cast<long long>(pol_bytes);
-        w.row_cap = ctx->row_cap;
-        w.queue_cap = ctx->queue_cap;
-        w.hash_cap = ctx->hash_cap;
+        set_lists(w, static_cast<int*>(ctx->fs_counters.ptr), static_cast<int*>(ctx->fs_ir.ptr),
+                  static_cast<int*>(ctx->fs_retry.ptr), kChunk, kChunk);
         w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr) + c0;
-        w.retry_pass = 0;
-        w.retry_cart = static_cast<int*>(ctx->fs_retry.ptr);
-        w.retry_polar = w.retry_cart + kChunk;
-        w.cand_cap = ctx->cand_cap;
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
-        // Too few inverse-ray points to fill the GPU with one warp per point (a
-        // single light curve, say, or a large batch that is mostly point
-        // sources) run every point on a whole block.
-        w.cell_budget = ctx->cell_budget;
-        w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
-        if (!ctx->check("counters", cudaMemsetAsync(counters, 0, 64 * sizeof(int), ctx->stream))) return false;
-        cudaEvent_t ev;
-        ctx->stage_begin(1, &ev);
-        if (!ctx->check("decide", launch_decide(w, ctx->sm_count, ctx->stream))) return false;
-        ctx->stage_end(1, ev);
-        const int warps = ctx->fs_warps < cn ? ctx->fs_warps : cn;
-        // Candidate keys and probes share one allocation: all warps' keys, then all probes.
-        const size_t per = seed_candidate_bytes_per_warp(ctx->cand_cap);
-        const size_t key_bytes = per * 8 / (8 + 16);
-        char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
-        ctx->stage_begin(2, &ev);
-        if (!ctx->check("seeds", launch_seeds(w, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
-                                              reinterpret_cast<P2*>(cb + key_bytes * ctx->fs_warps), warps)))
-            return false;
-        ctx->stage_end(2, ev);
-        if (++ctx->epoch >= 0xfff0ull) {
-            ctx->big_ready = false;
-            if (!ensure_big_scratch(ctx)) return false;
-            if (!ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart_bytes * ctx->fs_warps,
-                                                             ctx->stream)) ||
-                !ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff,
-                                                             pol_bytes * ctx->fs_warps, ctx->stream)))
-                return false;
-            ctx->epoch = 1;
-        }
-        ctx->stage_begin(3, &ev);
-        if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
-        ctx->stage_end(3, ev);
-        ctx->stage_begin(4, &ev);
-        if (ctx->polar_tiles) {
-            if (!ctx->check("polar", launch_polar_tiles(w, ctx->fs_tiles.ptr, ctx->tile_capacity, cn,
-                                                        ctx->tile_blocks, ctx->stream)))
-                return false;
-        } else if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) {
-            return false;
-        }
-        ctx->stage_end(4, ev);
-        // Second pass, one block per point, over the points that passed the cell
-        // budget or outgrew the first pass's scratch.
-        FsWork r = w;
-        r.retry_pass = 1;
-        r.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
-        r.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
-        r.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar_big.ptr);
-        r.scratch_polar_per_warp = static_cast<long long>(polar_bytes_big(ctx));
-        r.row_cap = ctx->row_cap_big;
-        r.queue_cap = ctx->queue_cap_big;
-        r.hash_cap = ctx->hash_cap_big;
-        ctx->stage_begin(3, &ev);
-        if (!ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
-        ctx->stage_end(3, ev);
-        ctx->stage_begin(4, &ev);
-        if (!ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
-        ctx->stage_end(4, ev);
-        ctx->launches += 2;
-        ctx->launches += 6;
+        if (!stage_decide(ctx, w) || !stage_seeds(ctx, w, cn) || !stage_integrate(ctx, w, cn)) return false;
         if (grads) {
             if (!ctx->ensure(ctx->fs_grad_tiles, grad_tile_bytes(ctx->tile_capacity, kChunk))) return false;
             if (ctx->grad_blocks == 0) ctx->grad_blocks = grad_flood_blocks_per_sm() * ctx->sm_count;
@@ -701,6 +763,32 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* sett
 
 namespace lcbi {
 
+// Grows b to at least `bytes`, keeping its contents (stream-ordered copy).
+bool grow_keep(Context* ctx, Buffer& b, size_t bytes)
+{
+    if (b.bytes >= bytes) return true;
+    Buffer nb;
+    size_t want = b.bytes * 2 > bytes ? b.bytes * 2 : bytes;
+    want = (want + 0xffff) & ~size_t(0xffff);
+    if (!ctx->check("cudaMalloc", cudaMalloc(&nb.ptr, want))) return false;
+    nb.bytes = want;
+    if (b.ptr) {
+        if (!ctx->check("store copy", cudaMemcpyAsync(nb.ptr, b.ptr, b.bytes, cudaMemcpyDeviceToDevice, ctx->stream)))
+            return false;
+        cudaFree(b.ptr);  // waits for the copy
+    }
+    b = nb;
+    return true;
+}
+
+// Large batches in which every point may have its own separation (lens
+// orbital motion): the caustic sampling and the decision run pass by pass, a
+// pass's caustic samples being dropped once it is decided, and the few
+// inverse-ray points of all passes are seeded and integrated together at the
+// end, so that no pass waits for its slowest inverse-ray point.  Two passes
+// are in flight: while the GPU samples and decides pass p, the host collects
+// the inverse-ray points of pass p - 1 and has their caustic models copied
+// into a store that outlives the pass.
 int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int n_settings,
                       const lcbi_fs_point* points, long long n, lcbi_fs_result* results, double* a_ps,
                       int32_t* image_count)
@@ -708,47 +796,204 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
     Context* ctx = reinterpret_cast<Context*>(c);
     if (!ctx || n < 0 || !settings || n_settings <= 0) return LCBI_INVALID_ARGUMENT;
     if (n == 0) return LCBI_OK;
-    if (!points || !results || !a_ps || !image_count) return LCBI_INVALID_ARGUMENT;
+    if (!points || !results || !a_ps || !image_count || n > (1ll << 30)) return LCBI_INVALID_ARGUMENT;
     for (long long i = 0; i < n; ++i)
         if (points[i].settings < 0 || points[i].settings >= n_settings) return LCBI_INVALID_ARGUMENT;
     ctx->error.clear();
     cudaSetDevice(ctx->device);
     if (!check_settings(ctx, settings, n_settings)) return LCBI_UNSUPPORTED;
-    if (!ctx->ensure(ctx->fs_all_out, n * sizeof(FsOut)) || !ctx->ensure(ctx->fs_all_aps, n * sizeof(double)) ||
-        !ctx->ensure(ctx->fs_all_nimg, n * sizeof(int)))
-        return LCBI_GPU_ERROR;
-    FsOut* all_out = static_cast<FsOut*>(ctx->fs_all_out.ptr);
-    double* all_aps = static_cast<double*>(ctx->fs_all_aps.ptr);
-    int* all_nimg = static_cast<int*>(ctx->fs_all_nimg.ptr);
-    std::vector<FsItem> items;
-    for (long long e0 = 0; e0 < n; e0 += kChunk) {
-        const long long cn = (n - e0) < kChunk ? (n - e0) : kChunk;
-        Plan plan;
-        add_settings(plan, settings, n_settings);
-        ModelTable mt{&plan};
-        items.resize(static_cast<size_t>(cn));
-        std::memcpy(items.data(), points + e0, cn * sizeof(FsItem));
-        for (auto& it : items) {
+
+    // Host: the points and every pass's caustic models (indices relative to the pass).
+    const long long n_pass = (n + kChunk - 1) / kChunk;
+    std::vector<FsItem> items(static_cast<size_t>(n));
+    std::memcpy(items.data(), points, n * sizeof(FsItem));
+    Plan plan;
+    add_settings(plan, settings, n_settings);
+    ModelTable mt{&plan};
+    std::vector<int> model_base(static_cast<size_t>(n_pass + 1));
+    long long max_raw = 0;
+    for (long long p = 0; p < n_pass; ++p) {
+        mt.restart_pass();
+        model_base[p] = static_cast<int>(plan.models.size());
+        const long long e1 = (p + 1) * kChunk < n ? (p + 1) * kChunk : n;
+        for (long long i = p * kChunk; i < e1; ++i) {
+            FsItem& it = items[i];
             const lcbi_fs_settings& st = settings[it.settings];
             it.a_ps = 0.0;
             it.flags = kItemPsExact | kItemSeedHints;
-            it.model = (it.rho > 0.0 && st.finite_mode > 0) ? mt.get_sequential(it.s, it.q, st.caustic_bins) : 0;
+            it.model = (it.rho > 0.0 && st.finite_mode > 0)
+                           ? mt.get_sequential(it.s, it.q, st.caustic_bins) - model_base[p]
+                           : 0;
         }
-        if (!upload(ctx, ctx->fs_items, items) || !ctx->ensure(ctx->fs_out, cn * sizeof(FsOut))) return LCBI_GPU_ERROR;
-        if (!ctx->check("images", launch_item_images(static_cast<FsItem*>(ctx->fs_items.ptr), cn, all_aps + e0,
-                                                     all_nimg + e0, ctx->sm_count, ctx->stream)))
-            return LCBI_GPU_ERROR;
-        ctx->launches += 1;
-        if (!run_pipeline(ctx, plan, cn)) return LCBI_GPU_ERROR;
-        if (!ctx->check("results D2D", cudaMemcpyAsync(all_out + e0, ctx->fs_out.ptr, cn * sizeof(FsOut),
-                                                       cudaMemcpyDeviceToDevice, ctx->stream)))
+        if (mt.raw_total > max_raw) max_raw = mt.raw_total;
+    }
+    model_base[n_pass] = static_cast<int>(plan.models.size());
+
+    // Device: tables, all points and their point-source values.
+    if (!prepare_tables(ctx, plan) || !prepare_counts(ctx, n) || !upload(ctx, ctx->fs_items, items) ||
+        !ctx->ensure(ctx->fs_out, n * sizeof(FsOut)) || !ctx->ensure(ctx->fs_all_aps, n * sizeof(double)) ||
+        !ctx->ensure(ctx->fs_all_nimg, n * sizeof(int)))
+        return LCBI_GPU_ERROR;
+    FsItem* d_items = static_cast<FsItem*>(ctx->fs_items.ptr);
+    FsOut* d_out = static_cast<FsOut*>(ctx->fs_out.ptr);
+    CausticModel* d_models = static_cast<CausticModel*>(ctx->fs_models.ptr);
+    const long long* d_ro = static_cast<const long long*>(ctx->fs_raw_offset.ptr);
+    if (!ctx->check("images", launch_item_images(d_items, n, static_cast<double*>(ctx->fs_all_aps.ptr),
+                                                 static_cast<int*>(ctx->fs_all_nimg.ptr), ctx->sm_count, ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+
+    // Pass buffers (two sets) and page-locked staging of their lists and jobs.
+    const size_t list_ints = 2 * static_cast<size_t>(kChunk);
+    const size_t job_bytes = static_cast<size_t>(kChunk) * (sizeof(StashJob) + sizeof(StashRemap));
+    const size_t stage_bytes = (64 + list_ints) * sizeof(int) + job_bytes;
+    for (int k = 0; k < 2; ++k) {
+        if (!ctx->ensure(ctx->pass_raw[k], (max_raw + 1) * sizeof(P2)) ||
+            !ctx->ensure(ctx->pass_branches[k], (max_raw + 1) * sizeof(P2)) ||
+            !ctx->ensure(ctx->pass_lists[k], list_ints * sizeof(int)) ||
+            !ctx->ensure(ctx->pass_counters[k], 64 * sizeof(int)) || !ctx->ensure(ctx->pass_jobs[k], job_bytes))
             return LCBI_GPU_ERROR;
     }
-    if (!ctx->check("results D2H", cudaMemcpyAsync(results, all_out, n * sizeof(lcbi_fs_result),
+    if (ctx->pinned_bytes < 2 * stage_bytes) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        if (!ctx->check("cudaMallocHost", cudaMallocHost(&ctx->pinned, 2 * stage_bytes))) return LCBI_GPU_ERROR;
+        ctx->pinned_bytes = 2 * stage_bytes;
+    }
+    auto stage_of = [&](int k) { return static_cast<char*>(ctx->pinned) + k * stage_bytes; };
+    cudaEvent_t pass_done[2];
+    for (int k = 0; k < 2; ++k)
+        if (!ctx->check("event", cudaEventCreateWithFlags(&pass_done[k], cudaEventDisableTiming))) return LCBI_GPU_ERROR;
+    struct Events {
+        cudaEvent_t* e;
+        ~Events() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); }
+    } events_guard{pass_done};
+
+    std::vector<int> g_cart, g_polar;
+    long long store_models = 0, store_points = 0;
+    std::vector<int> dst_of;  // per model of the pass being collected: store index, or -1
+
+    auto enqueue_pass = [&](long long p) -> bool {
+        const int k = static_cast<int>(p & 1);
+        const long long c0 = p * kChunk;
+        const int cn = static_cast<int>((n - c0) < kChunk ? (n - c0) : kChunk);
+        const int base = model_base[p];
+        const int nmod = model_base[p + 1] - base;
+        cudaEvent_t ev;
+        ctx->stage_begin(0, &ev);
+        if (nmod > 0) {
+            if (!ctx->check("caustics", launch_caustics(d_models + base, nmod, plan.max_bins,
+                                                        static_cast<double2*>(ctx->fs_phases.ptr), d_ro + base,
+                                                        static_cast<P2*>(ctx->pass_raw[k].ptr),
+                                                        static_cast<P2*>(ctx->pass_branches[k].ptr), ctx->stream)))
+                return false;
+            ctx->launches += 2;
+        }
+        ctx->stage_end(0, ev);
+        FsWork w = common_work(ctx);
+        w.items = d_items + c0;
+        w.models = d_models + base;
+        w.raw_offset = d_ro + base;
+        w.raw = static_cast<const P2*>(ctx->pass_raw[k].ptr);
+        w.branches = static_cast<const P2*>(ctx->pass_branches[k].ptr);
+        w.out = d_out + c0;
+        w.n_items = cn;
+        set_lists(w, static_cast<int*>(ctx->pass_counters[k].ptr), static_cast<int*>(ctx->pass_lists[k].ptr),
+                  nullptr, kChunk, 0);
+        w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr) + c0;
+        w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
+        if (!stage_decide(ctx, w)) return false;
+        int* st = reinterpret_cast<int*>(stage_of(k));
+        return ctx->check("lists D2H", cudaMemcpyAsync(st, ctx->pass_counters[k].ptr, 64 * sizeof(int),
+                                                       cudaMemcpyDeviceToHost, ctx->stream)) &&
+               ctx->check("lists D2H", cudaMemcpyAsync(st + 64, ctx->pass_lists[k].ptr, list_ints * sizeof(int),
+                                                       cudaMemcpyDeviceToHost, ctx->stream)) &&
+               ctx->check("event", cudaEventRecord(pass_done[k], ctx->stream));
+    };
+
+    auto collect_pass = [&](long long p) -> bool {
+        const int k = static_cast<int>(p & 1);
+        const long long c0 = p * kChunk;
+        const int base = model_base[p];
+        if (!ctx->check("pass wait", cudaEventSynchronize(pass_done[k]))) return false;
+        const int* st = reinterpret_cast<const int*>(stage_of(k));
+        const int nc = st[0], np = st[1];
+        const int* lists = st + 64;
+        StashJob* jobs = reinterpret_cast<StashJob*>(stage_of(k) + (64 + list_ints) * sizeof(int));
+        StashRemap* remaps = reinterpret_cast<StashRemap*>(jobs + kChunk);
+        dst_of.assign(static_cast<size_t>(model_base[p + 1] - base), -1);
+        int n_jobs = 0, n_remaps = 0;
+        for (int j = 0; j < nc + np; ++j) {
+            const int it = j < nc ? lists[j] : lists[kChunk + (j - nc)];
+            const long long g = c0 + it;
+            const int m = items[g].model;
+            if (dst_of[m] < 0) {
+                dst_of[m] = static_cast<int>(store_models++);
+                jobs[n_jobs++] = StashJob{m, dst_of[m], store_points};
+                store_points += 4ll * plan.models[base + m].bins;
+            }
+            remaps[n_remaps++] = StashRemap{g, dst_of[m], 0};
+            (j < nc ? g_cart : g_polar).push_back(static_cast<int>(g));
+        }
+        if (n_jobs == 0) return true;
+        if (!grow_keep(ctx, ctx->ir_models, (size_t)store_models * sizeof(CausticModel)) ||
+            !grow_keep(ctx, ctx->ir_branches, (size_t)store_points * sizeof(P2)))
+            return false;
+        char* dj = static_cast<char*>(ctx->pass_jobs[k].ptr);
+        if (!ctx->check("jobs H2D", cudaMemcpyAsync(dj, jobs, n_jobs * sizeof(StashJob), cudaMemcpyHostToDevice,
+                                                    ctx->stream)) ||
+            !ctx->check("jobs H2D", cudaMemcpyAsync(dj + kChunk * sizeof(StashJob), remaps,
+                                                    n_remaps * sizeof(StashRemap), cudaMemcpyHostToDevice,
+                                                    ctx->stream)))
+            return false;
+        ctx->launches += 1;
+        return ctx->check("stash", launch_stash(d_models + base, static_cast<const P2*>(ctx->pass_branches[k].ptr),
+                                                reinterpret_cast<const StashJob*>(dj), n_jobs,
+                                                static_cast<CausticModel*>(ctx->ir_models.ptr),
+                                                static_cast<P2*>(ctx->ir_branches.ptr),
+                                                reinterpret_cast<const StashRemap*>(dj + kChunk * sizeof(StashJob)),
+                                                n_remaps, d_items, ctx->stream));
+    };
+
+    for (long long p = 0; p < n_pass; ++p) {
+        if (!enqueue_pass(p)) return LCBI_GPU_ERROR;
+        if (p > 0 && !collect_pass(p - 1)) return LCBI_GPU_ERROR;
+    }
+    if (!collect_pass(n_pass - 1)) return LCBI_GPU_ERROR;
+
+    // All inverse-ray points: seeds, then the integration.
+    const int n_cart = static_cast<int>(g_cart.size());
+    const int n_polar = static_cast<int>(g_polar.size());
+    const int n_ir = n_cart + n_polar;
+    if (n_ir > 0) {
+        std::vector<int> lists(g_cart);
+        lists.insert(lists.end(), g_polar.begin(), g_polar.end());
+        std::vector<int> counters(64, 0);
+        counters[0] = n_cart;
+        counters[1] = n_polar;
+        if (!upload(ctx, ctx->ir_lists, lists) || !upload(ctx, ctx->ir_counters, counters) ||
+            !ctx->ensure(ctx->ir_retry, (size_t)2 * n_ir * sizeof(int)) ||
+            !ctx->ensure(ctx->fs_seeds, (size_t)n_ir * ctx->seed_cap * sizeof(P2)) ||
+            !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, n_ir)))
+            return LCBI_GPU_ERROR;
+        FsWork w = common_work(ctx);
+        w.items = d_items;
+        w.models = static_cast<const CausticModel*>(ctx->ir_models.ptr);
+        w.branches = static_cast<const P2*>(ctx->ir_branches.ptr);
+        w.out = d_out;
+        w.n_items = 0;
+        set_lists(w, static_cast<int*>(ctx->ir_counters.ptr), static_cast<int*>(ctx->ir_lists.ptr),
+                  static_cast<int*>(ctx->ir_retry.ptr), n_cart, n_ir);
+        w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr);
+        w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) : nullptr;
+        if (!stage_seeds(ctx, w, n_ir) || !stage_integrate(ctx, w, n_ir)) return LCBI_GPU_ERROR;
+    }
+    if (!ctx->check("results D2H", cudaMemcpyAsync(results, d_out, n * sizeof(lcbi_fs_result),
                                                    cudaMemcpyDeviceToHost, ctx->stream)) ||
-        !ctx->check("a_ps D2H", cudaMemcpyAsync(a_ps, all_aps, n * sizeof(double), cudaMemcpyDeviceToHost,
+        !ctx->check("a_ps D2H", cudaMemcpyAsync(a_ps, ctx->fs_all_aps.ptr, n * sizeof(double), cudaMemcpyDeviceToHost,
                                                 ctx->stream)) ||
-        !ctx->check("images D2H", cudaMemcpyAsync(image_count, all_nimg, n * sizeof(int32_t),
+        !ctx->check("images D2H", cudaMemcpyAsync(image_count, ctx->fs_all_nimg.ptr, n * sizeof(int32_t),
                                                   cudaMemcpyDeviceToHost, ctx->stream)) ||
         !ctx->finish())
         return LCBI_GPU_ERROR;

@@ -62,9 +62,18 @@ __device__ __forceinline__ void perm_of_rank(int r, int* p)
 
 __device__ __forceinline__ bool angle_less(P2 l, P2 r) { return atan2(l.y, l.x) < atan2(r.y, r.x); }
 
+// The 24 permutations of {0, 1, 2, 3} in lexicographic order (the order
+// std::next_permutation visits from the identity), packed two bits per entry:
+// entry b of permutation r is (kPermCode[r] >> 2b) & 3.
+__constant__ unsigned char kPermCode[24] = {228, 180, 216, 120, 156, 108, 225, 177, 201, 57, 141, 45,
+                                            210, 114, 198, 54,  78,  30,  147, 99,  135, 39, 75,  27};
+
+constexpr int kTrackBatch = 64;                      // samples staged per batch
+constexpr int kTrackLoads = 4 * kTrackBatch / 32;    // points each lane loads per batch
+
 __global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models, int n_models,
                                                           const long long* __restrict__ raw_offset,
-                                                          const P2* __restrict__ raw, P2* branches)
+                                                          const P2* __restrict__ raw, P2* __restrict__ branches)
 {
     const int m = blockIdx.x;
     if (m >= n_models) return;
@@ -92,6 +101,7 @@ __global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models,
     // by the first minimum-cost permutation in lexicographic order.
     int perm[4];
     perm_of_rank(lane < 24 ? lane : 0, perm);
+    const unsigned my_code = kPermCode[lane < 24 ? lane : 0];
     P2 end[4];
     {
         P2 v[4] = {pts[0], pts[1], pts[2], pts[3]};
@@ -108,46 +118,63 @@ __global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models,
         for (int b = 0; b < 4; ++b) end[b] = v[b];
         if (lane < 4) br[(long long)lane * bins] = v[lane];
     }
+    // The samples are consumed strictly in order, one step (4 points) at a
+    // time, and each step's assignment depends on the previous one; so the
+    // points are staged in shared memory kTrackBatch steps at a time, the
+    // next batch being loaded into registers while the current one is
+    // consumed, which keeps the memory latency off the serial chain.
+    __shared__ P2 stage[4 * kTrackBatch];
+    P2 nxt[kTrackLoads];
+    auto load_batch = [&](int s0) {
+        const long long first = 4ll * s0, last = 4ll * bins;
+#pragma unroll
+        for (int u = 0; u < kTrackLoads; ++u) {
+            const long long j = first + lane + 32 * u;
+            if (j < last) nxt[u] = pts[j];
+        }
+    };
     double max_seg2 = 0.0;
-    for (int i = 1; i < bins; ++i) {
-        const P2* cur = pts + 4ll * i;
-        P2 c[4] = {cur[0], cur[1], cur[2], cur[3]};
+    load_batch(1);
+    for (int s0 = 1; s0 < bins; s0 += kTrackBatch) {
+        const int s1 = min(bins, s0 + kTrackBatch);
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < kTrackLoads; ++u) {
+            const int j = lane + 32 * u;
+            if (j < 4 * (s1 - s0)) stage[j] = nxt[u];
+        }
+        __syncwarp();
+        if (s1 < bins) load_batch(s1);
+    for (int i = s0; i < s1; ++i) {
+        const P2* cur = stage + 4 * (i - s0);
         double cost = 0.0;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            P2 sel = c[0];
+        for (int b = 0; b < 4; ++b) cost += dist2(end[b], cur[perm[b]]);
+        // The first permutation of least cost: a butterfly over (cost, rank),
+        // ties going to the lower rank; a cost that is not below +inf (NaN
+        // included) never wins, and with none below +inf rank 0 does, as in a
+        // serial scan with a strict comparison.
+        double best = (lane < 24 && cost < dinf()) ? cost : dinf();
+        int bp = lane < 24 ? lane : 32 + lane;
 #pragma unroll
-            for (int k = 1; k < 4; ++k)
-                if (perm[b] == k) sel = c[k];
-            cost += dist2(end[b], sel);
-        }
-        double best = dinf();
-        int bp = 0;
-        for (int r = 0; r < 24; ++r) {
-            const double cr = shfl_d(cost, r);
-            if (cr < best) {
-                best = cr;
-                bp = r;
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int op = __shfl_xor_sync(0xffffffffu, bp, off);
+            if (ob < best || (ob == best && op < bp)) {
+                best = ob;
+                bp = op;
             }
         }
-        int pb[4];
-        perm_of_rank(bp, pb);
+        const unsigned code = __shfl_sync(0xffffffffu, my_code, bp);
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            P2 sel = c[0];
-#pragma unroll
-            for (int k = 1; k < 4; ++k)
-                if (pb[b] == k) sel = c[k];
+            const P2 sel = cur[(code >> (2 * b)) & 3u];
             const double seg2 = dist2(end[b], sel);
             if (seg2 > max_seg2) max_seg2 = seg2;
             end[b] = sel;
         }
-        if (lane < 4) {
-            P2 sel = c[0];
-            for (int k = 1; k < 4; ++k)
-                if (pb[lane] == k) sel = c[k];
-            br[(long long)lane * bins + i] = sel;
-        }
+        if (lane < 4) br[(long long)lane * bins + i] = cur[(code >> (2 * lane)) & 3u];
+    }
     }
     if (lane == 0) {
         md.min_x = mnx;

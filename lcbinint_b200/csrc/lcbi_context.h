@@ -33,7 +33,14 @@ struct Context {
     Buffer fs_ir, fs_counters, fs_seeds, fs_cand_keys, fs_cand_probes, fs_scratch, fs_scratch_polar;
     Buffer fs_trig, fs_lc_models, fs_times, fs_ld_coeffs, fs_rays, fs_retry, fs_scratch_big, fs_scratch_polar_big;
     Buffer fs_cycles, fs_tiles, fs_grad_tiles, fs_grad, fs_grad_lc;
-    Buffer fs_all_out, fs_all_aps, fs_all_nimg;  // whole-batch results of binary_mag_images
+    Buffer fs_all_aps, fs_all_nimg;  // whole-batch point-source values of binary_mag_images
+    // binary_mag_images: caustic samples and work lists of two passes in
+    // flight, and the store of what the inverse-ray points need after their
+    // pass (their caustic models, work lists and seeds).
+    Buffer pass_raw[2], pass_branches[2], pass_lists[2], pass_counters[2], pass_jobs[2];
+    Buffer ir_models, ir_branches, ir_lists, ir_counters, ir_retry;
+    void* pinned = nullptr;     // page-locked staging of the passes' work lists and jobs
+    size_t pinned_bytes = 0;
     bool trig_ready = false;
     unsigned long long epoch = 0;
     int fs_warps = 0;          // persistent warps the scratch areas are sized for
@@ -83,7 +90,9 @@ struct Context {
                           &fs_branches, &fs_ld, &fs_ir, &fs_counters, &fs_seeds, &fs_cand_keys, &fs_cand_probes,
                           &fs_scratch, &fs_scratch_polar, &fs_trig, &fs_lc_models, &fs_times, &fs_ld_coeffs,
                           &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc,
-                          &fs_all_out, &fs_all_aps, &fs_all_nimg})
+                          &fs_all_aps, &fs_all_nimg, &pass_raw[0], &pass_raw[1], &pass_branches[0],
+                          &pass_branches[1], &pass_lists[0], &pass_lists[1], &pass_counters[0], &pass_counters[1],
+                          &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry})
             v.push_back(b);
         return v;
     }

@@ -126,6 +126,22 @@ struct LcModel {
 };
 cudaError_t launch_lc_items(const LcModel* models, int n_models, const double* times, FsItem* items,
                             long long n_items, cudaStream_t stream);
+// What an inverse-ray point needs after its pass of the deferred pipeline:
+// its caustic model copied from the pass's tables into the inverse-ray store
+// (jobs), and the point's model index pointed at the copy (remaps).
+struct StashJob {
+    int src_model;          // index in the pass's model table
+    int dst_model;          // index in the store
+    long long dst_offset;   // first branch point of the copy in the store
+};
+struct StashRemap {
+    long long item;         // index of the point in the whole batch
+    int dst_model;
+    int pad;
+};
+cudaError_t launch_stash(const CausticModel* src_models, const P2* src_branches, const StashJob* jobs, int n_jobs,
+                         CausticModel* dst_models, P2* dst_branches, const StashRemap* remaps, int n_remaps,
+                         FsItem* items, cudaStream_t stream);
 // a_ps and image count per item from binary_images (rho > 0) or binary_mag0
 // (rho == 0), written into the items and into a_ps[n], nimg[n].
 cudaError_t launch_item_images(FsItem* items, long long n, double* a_ps, int* nimg, int sm_count, cudaStream_t stream);

@@ -842,6 +842,18 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
                                                  static_cast<int*>(ctx->fs_all_nimg.ptr), ctx->sm_count, ctx->stream)))
         return LCBI_GPU_ERROR;
     ctx->launches += 1;
+    // Points that provably take the decision's bounding-box exit need no
+    // caustic samples; only the models of the others are sampled.
+    const size_t n_models_all = plan.models.size();
+    if (!upload(ctx, ctx->fs_model_base, model_base) || !ctx->ensure(ctx->fs_needed, n_models_all + 1) ||
+        !ctx->check("needed init", cudaMemsetAsync(ctx->fs_needed.ptr, 0, n_models_all + 1, ctx->stream)) ||
+        !ctx->check("certify", launch_certify(d_items, n, static_cast<const FsSettingsDev*>(ctx->fs_settings.ptr),
+                                              static_cast<const int*>(ctx->fs_model_base.ptr), kChunk,
+                                              static_cast<unsigned char*>(ctx->fs_needed.ptr), ctx->sm_count,
+                                              ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    const unsigned char* d_needed = static_cast<const unsigned char*>(ctx->fs_needed.ptr);
 
     // Pass buffers (two sets) and page-locked staging of their lists and jobs.
     const size_t list_ints = 2 * static_cast<size_t>(kChunk);
@@ -886,7 +898,8 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
             if (!ctx->check("caustics", launch_caustics(d_models + base, nmod, plan.max_bins,
                                                         static_cast<double2*>(ctx->fs_phases.ptr), d_ro + base,
                                                         static_cast<P2*>(ctx->pass_raw[k].ptr),
-                                                        static_cast<P2*>(ctx->pass_branches[k].ptr), ctx->stream)))
+                                                        static_cast<P2*>(ctx->pass_branches[k].ptr), ctx->stream,
+                                                        d_needed + base)))
                 return false;
             ctx->launches += 2;
         }

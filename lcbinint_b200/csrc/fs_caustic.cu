@@ -27,11 +27,12 @@ __global__ void ld_table_kernel(const double2* __restrict__ coeffs, int n_tables
 
 __global__ void __launch_bounds__(128) caustic_roots_kernel(const CausticModel* __restrict__ models, int n_models,
                                                            const double2* __restrict__ phases,
-                                                           const long long* __restrict__ raw_offset, P2* raw)
+                                                           const long long* __restrict__ raw_offset, P2* raw,
+                                                           const unsigned char* __restrict__ needed)
 {
     // Flattened (model, phase) index; models are laid out back to back.
     const int m = blockIdx.y;
-    if (m >= n_models) return;
+    if (m >= n_models || (needed && !needed[m])) return;
     const CausticModel md = models[m];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < md.bins; i += gridDim.x * blockDim.x) {
         const double2 ph = phases[md.phase_offset + i];
@@ -73,10 +74,11 @@ constexpr int kTrackLoads = 4 * kTrackBatch / 32;    // points each lane loads p
 
 __global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models, int n_models,
                                                           const long long* __restrict__ raw_offset,
-                                                          const P2* __restrict__ raw, P2* __restrict__ branches)
+                                                          const P2* __restrict__ raw, P2* __restrict__ branches,
+                                                          const unsigned char* __restrict__ needed)
 {
     const int m = blockIdx.x;
-    if (m >= n_models) return;
+    if (m >= n_models || (needed && !needed[m])) return;
     const int lane = lane_id();
     CausticModel md = models[m];
     const int bins = md.bins;
@@ -199,14 +201,15 @@ cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables
 }
 
 cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,
-                            const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream)
+                            const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream,
+                            const unsigned char* needed)
 {
     if (n_models <= 0) return cudaSuccess;
     dim3 grid((max_bins + 127) / 128, n_models);
-    caustic_roots_kernel<<<grid, 128, 0, stream>>>(models, n_models, phases, raw_offset, raw);
+    caustic_roots_kernel<<<grid, 128, 0, stream>>>(models, n_models, phases, raw_offset, raw, needed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    caustic_track_kernel<<<n_models, 32, 0, stream>>>(models, n_models, raw_offset, raw, branches);
+    caustic_track_kernel<<<n_models, 32, 0, stream>>>(models, n_models, raw_offset, raw, branches, needed);
     return cudaGetLastError();
 }
 

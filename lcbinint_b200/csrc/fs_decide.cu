@@ -57,6 +57,10 @@ __global__ void __launch_bounds__(128) decide_kernel(FsWork w)
             o.A = shfl_d(a, 0);
         } else if (st.finite_mode <= 0) {
             o.A = a_ps;
+        } else if (item.flags & kItemOutsideBox) {
+            // Outside the outer caustic box by the margin, hence outside the
+            // sampled caustic's bounding box by it: the bounding-box exit.
+            o.A = a_ps;
         } else {
             const CausticModel md = w.models[item.model];
             const P2* raw = w.raw + w.raw_offset[item.model];
@@ -165,6 +169,40 @@ __global__ void __launch_bounds__(128) decide_kernel(FsWork w)
             w.out[it] = o;
         }
     }
+}
+
+__global__ void __launch_bounds__(128) certify_kernel(FsItem* __restrict__ items, long long n,
+                                                     const FsSettingsDev* __restrict__ settings,
+                                                     const int* __restrict__ model_base, int pass,
+                                                     unsigned char* __restrict__ needed)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const FsItem item = items[i];
+        const FsSettingsDev st = settings[item.settings];
+        if (!(item.rho > 0.0) || st.finite_mode <= 0) continue;
+        // The decision's margin (finite_source_magnifier.cpp:4679-4698).
+        const double margin = st.kinji_threshold * item.rho;
+        const bool adaptive = st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0);
+        const double amargin = adaptive ? dmax_(margin, 60.0 * item.rho) : margin;
+        const CausticBox b = caustic_outer_box(item.s, item.q);
+        if (b.ok && (item.x < b.lo_x - amargin || item.x > b.hi_x + amargin || item.y < -b.half_y - amargin ||
+                     item.y > b.half_y + amargin))
+            items[i].flags = item.flags | kItemOutsideBox;
+        else
+            needed[model_base[i / pass] + item.model] = 1;
+    }
+}
+
+cudaError_t launch_certify(FsItem* items, long long n, const FsSettingsDev* settings, const int* model_base, int pass,
+                           unsigned char* needed, int sm_count, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    long long blocks = (n + 127) / 128;
+    const long long cap = (long long)sm_count * 16;
+    if (blocks > cap) blocks = cap;
+    certify_kernel<<<(unsigned)blocks, 128, 0, stream>>>(items, n, settings, model_base, pass, needed);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_decide(const FsWork& w, int sm_count, cudaStream_t stream)

@@ -86,4 +86,75 @@ __device__ __forceinline__ double caustic_distance(const CausticModel& md, const
     return warp_min(d);
 }
 
+// A box that holds every point of a binary lens's caustic, from the lens
+// equation alone (no sampling), so that a source outside it by the decision's
+// margin is outside the sampled caustic's bounding box by that margin too
+// (the sampled points lie on the caustic).
+//
+// Lens frame of the sampled caustic: mass m1 (the heavier) at z = a, mass m2
+// at 0, a = -s or s; a critical point z has |m1/(z-a)^2 + m2/z^2| = 1 and maps
+// to w = z - m1/conj(z-a) - m2/conj(z).  Split the critical points by which
+// lens dominates, mn/dn^2 >= mf/df^2 (dn, df their distances to the near and
+// far lens).  Then
+//   dn <= sqrt(2 mn)                              (1 <= mn/dn^2 + mf/df^2),
+//   df >= max(s - sqrt(2 mn), s / (1 + sqrt(mn/mf)))   (dn + df >= s, dominance),
+//   mn/dn^2 <= 1 + e,  e = mf / df_min^2          (reverse triangle inequality),
+//   mn/dn^2 >= 1 - e   when e < 1,
+// and |w - zn| <= |dn - mn/dn| + mf/df, with |d - mn/d| increasing away from
+// sqrt(mn) so that its maximum over [dn_min, dn_max] is at an end.  When
+// dn_max < s the far lens's deflection is nearly constant near zn:
+// |w - (zn - mf/conj(zn - zf))| <= |dn - mn/dn| + mf dn_max / (s (s - dn_max)).
+// The smaller of the two discs about each lens is kept.
+struct CausticBox {
+    double lo_x, hi_x, half_y;  // source frame of the decision (the lens frame shifted by -a m1)
+    bool ok;
+};
+
+__device__ __forceinline__ void dominated_disc(double mn, double mf, double s, double zn, double shift, double* c,
+                                               double* r)
+{
+    double dmax = sqrt(2.0 * mn);
+    const double dfmin = fmax(s - dmax, s / (1.0 + sqrt(mn / mf)));
+    const double e = mf / (dfmin * dfmin);
+    const double dmin = sqrt(mn / (1.0 + e));
+    if (e < 1.0) dmax = fmin(dmax, sqrt(mn / (1.0 - e)));
+    const double core = fmax(fabs(dmin - mn / dmin), fabs(dmax - mn / dmax));
+    *c = zn;
+    *r = core + mf / dfmin;
+    if (dmax < s) {
+        const double r2 = core + mf * dmax / (s * (s - dmax));
+        if (r2 < *r) {
+            *c = zn - shift;
+            *r = r2;
+        }
+    }
+}
+
+__device__ __forceinline__ CausticBox caustic_outer_box(double separation, double mass_ratio)
+{
+    CausticBox b{0.0, 0.0, 0.0, false};
+    const double s = fabs(separation);
+    const double q_in = fabs(mass_ratio);
+    if (!(s > 0.0) || !(q_in > 0.0) || !isfinite(s) || !isfinite(q_in)) return b;
+    const double q = q_in < 1.0 ? q_in : 1.0 / q_in;
+    const double a = q_in < 1.0 ? -s : s;
+    const double m1 = 1.0 / (1.0 + q);
+    const double m2 = q * m1;
+    double c1, r1, c2, r2;
+    dominated_disc(m1, m2, s, a, m2 / a, &c1, &r1);     // near m1: far-lens deflection m2/conj(a - 0)
+    dominated_disc(m2, m1, s, 0.0, -m1 / a, &c2, &r2);  // near m2: far-lens deflection m1/conj(0 - a)
+    // Generous slack for the rounding of the sampled points and of this bound.
+    r1 = r1 * (1.0 + 1.0e-6) + 1.0e-9;
+    r2 = r2 * (1.0 + 1.0e-6) + 1.0e-9;
+    const double sh = a * m1;
+    b.lo_x = fmin(c1 - r1, c2 - r2) - sh;
+    b.hi_x = fmax(c1 + r1, c2 + r2) - sh;
+    const double pad = 1.0e-9 + 1.0e-9 * (fabs(b.lo_x) + fabs(b.hi_x));
+    b.lo_x -= pad;
+    b.hi_x += pad;
+    b.half_y = fmax(r1, r2);
+    b.ok = isfinite(b.lo_x) && isfinite(b.hi_x) && isfinite(b.half_y);
+    return b;
+}
+
 } // namespace lcbi

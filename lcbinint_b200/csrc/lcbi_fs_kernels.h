@@ -21,6 +21,7 @@ enum : int {
     kItemPsExact = 1,     // point_source_magnification_is_exact (hexadecapole reuses a_ps)
     kItemPsOnDevice = 2,  // a_ps = binary_mag0(s, q, x, y), computed by the decision kernel
     kItemSeedHints = 4,   // the point images are seed hints, kept only if they map inside the source
+    kItemOutsideBox = 8,  // set by launch_certify: the source is outside the outer caustic box by the margin
 };
 
 // Per-item outputs.
@@ -91,8 +92,15 @@ struct FsWork {
 constexpr int kBigWarps = 8;
 
 cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables, cudaStream_t stream);
+// needed (optional): models whose flag is 0 are not sampled.
 cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,
-                            const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream);
+                            const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream,
+                            const unsigned char* needed = nullptr);
+// Points (rho > 0, finite_mode > 0) whose source is outside the outer caustic
+// box (caustic_outer_box) by the decision's margin get kItemOutsideBox; the
+// others set needed[model_base[i / pass] + model].  needed must be zeroed.
+cudaError_t launch_certify(FsItem* items, long long n, const FsSettingsDev* settings, const int* model_base, int pass,
+                           unsigned char* needed, int sm_count, cudaStream_t stream);
 cudaError_t launch_decide(const FsWork& w, int sm_count, cudaStream_t stream);
 cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, long long* cand_keys, P2* cand_probes,
                          int n_warps);

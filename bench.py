@@ -654,9 +654,11 @@ def run_orbital(args, world, rank, local_rank, ncores, common):
     out.  The parallax half needs the reference's Earth ephemeris table,
     which is missing, so parallax is not applied."""
     dicts, modes, gams, times = orbital_workload(seed=3 + rank)
+    if args.models > 0:
+        dicts, modes, gams = dicts[:args.models], modes[:args.models], gams[:args.models]
     M, K = len(dicts), times.size
     n = M * K
-    config = {"workload": "orbital: 1024 models x 2000 epochs over 200 days, half circular / half Keplerian lens "
+    config = {"workload": f"orbital: {M} models x 2000 epochs over 200 days, half circular / half Keplerian lens "
                           "orbital motion (g1, g2 U[-1,1]/yr, g3 U[0,0.5]/yr), config-3 model distribution, "
                           "linear LD U[0,0.8], auto decision tree, nbin 50; parallax not applied (no ephemeris)",
               "points": n, "l2": "not flushed (per-epoch caustic samples, 2.9 GB per chunk, exceed L2)",
@@ -774,6 +776,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N points (small cases for profiler captures)")
+    ap.add_argument("--models", type=int, default=0,
+                    help="orbital workload: use only the first N models (small cases for profiler captures)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

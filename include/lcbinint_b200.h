@@ -237,6 +237,20 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *se
                                const double *times, int64_t n_times, double *A, double *dA, int32_t *method,
                                int32_t *status);
 
+/* Caustic (caustic != 0) or critical curve (caustic == 0) of a binary lens
+ * (python/lcbinint_pybind.cpp:1882-1926, LightCurve.caustics /
+ * critical_curves): the critical-curve quartic at n_points phases
+ * 2 pi i / n_points (n_points >= 8), its four roots, mapped through the lens
+ * equation for the caustic, tracked into four branches by the first
+ * least-cost assignment to each branch's last point (the first phase sorted
+ * by polar angle).  q is the core-convention mass ratio the magnification
+ * entry points take (1/q of VBM parameters); critical points are in the lens
+ * frame of the quartic (heavier mass at -s or s, lighter at the origin),
+ * caustic points in the source frame.  xy[2 * (b * n_points + j)] = (x, y) of
+ * point j of branch b; points_per_branch (optional) receives n_points. */
+int lcbi_gpu_binary_geometry(lcbi_gpu_context *ctx, double s, double q, int32_t n_points, int32_t caustic,
+                             double *xy, int32_t *points_per_branch);
+
 /* Lattice cells counted by the last finite-source call (one count per point,
  * cells whose centre maps inside the source disk), for ray-throughput
  * accounting; no reference counterpart.  n must not exceed that call's size. */
@@ -410,6 +424,16 @@ const char *lcbi_status_string(lcbi_status status);
  * only.  Returns LCBI_OK once every set has its status, else the error that
  * stopped the batch (LCBI_INVALID_ARGUMENT for bad array arguments,
  * LCBI_GPU_ERROR). */
+/* Lens orbital motion at `time` (src/lcbinint/model/orbital_motion.cpp:69-183;
+ * Python lcbinint.circular_orbital_motion / kepler_orbital_motion,
+ * python/lcbinint_pybind.cpp:3896-3925): state = {projected separation,
+ * angle of the binary axis, line-of-sight separation}.  Host arithmetic,
+ * bit-identical to the reference's. */
+int lcbi_circular_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
+                                 double reference_time, double *state);
+int lcbi_kepler_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
+                               double szs, double ar, double reference_time, double *state);
+
 #define LCBI_ARRAYS_KEYWORD_ROUTE 1u
 int lcbi_gpu_magnification_arrays(lcbi_gpu_context *ctx, int32_t n_sets, const lcbi_params *params,
                                   const lcbi_options *options, const int64_t *first, const int32_t *count,

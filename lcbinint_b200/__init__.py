@@ -11,8 +11,10 @@ import numpy as np
 
 from . import _lib
 from ._lib import GpuError, LibraryMissing, context
-from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, LightCurve, LightCurveFunc, LightCurveInfo,
-                  LimbDarkening, Options, binary_inverse_ray, binary_inverse_ray_batch, binary_mag, light_curves)
+from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, GeometryBranches, LightCurve, LightCurveFunc,
+                  LightCurveInfo, LimbDarkening, Options, binary_geometry, binary_inverse_ray,
+                  binary_inverse_ray_batch, binary_mag, circular_orbital_motion, kepler_orbital_motion, light_curves,
+                  magnification_arrays)
 
 __all__ = [
     "binary_mag0",
@@ -21,6 +23,11 @@ __all__ = [
     "binary_inverse_ray_batch",
     "binary_mag",
     "light_curves",
+    "magnification_arrays",
+    "binary_geometry",
+    "GeometryBranches",
+    "circular_orbital_motion",
+    "kepler_orbital_motion",
     "LightCurve",
     "LightCurveFunc",
     "LightCurveInfo",

@@ -354,6 +354,43 @@ STATIC = 0
 CIRCULAR = 1
 KEPLER = 2
 
+
+def circular_orbital_motion(time, separation, angle, g1=0.0, g2=0.0, g3=0.0, reference_time=0.0):
+    """lcbinint.circular_orbital_motion (PYB:3896-3908): (separation, angle,
+    line-of-sight separation) of a circular lens orbit at `time`."""
+    out = np.zeros(3)
+    _lib.lib().lcbi_circular_orbital_motion(float(time), float(separation), float(angle), float(g1), float(g2),
+                                            float(g3), float(reference_time), _lib.ptr(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+def kepler_orbital_motion(time, separation, angle, g1=0.0, g2=0.0, g3=0.0, szs=0.0, ar=1.0, reference_time=0.0):
+    """lcbinint.kepler_orbital_motion (PYB:3910-3925): the Keplerian counterpart."""
+    out = np.zeros(3)
+    _lib.lib().lcbi_kepler_orbital_motion(float(time), float(separation), float(angle), float(g1), float(g2),
+                                          float(g3), float(szs), float(ar), float(reference_time), _lib.ptr(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+@dataclass
+class GeometryBranches:
+    """lcbinint.GeometryBranches (PYB:51-54, 2811-2813): four tracked branches."""
+    x: list = field(default_factory=list)
+    y: list = field(default_factory=list)
+
+
+def binary_geometry(s: float, q_core: float, n_points: int, caustic: bool, *, device: int = 0) -> GeometryBranches:
+    """Caustic or critical-curve branches of a binary lens (lcbi_gpu_binary_geometry)."""
+    if int(n_points) < 8:
+        raise ValueError("n_points must be at least 8")
+    n = int(n_points)
+    xy = np.empty((4, n, 2))
+    ctx = context(device)
+    rc = ctx._L.lcbi_gpu_binary_geometry(ctx.handle, float(s), float(q_core), n, 1 if caustic else 0,
+                                         _lib.ptr(xy), None)
+    ctx.check(rc, "lcbi_gpu_binary_geometry")
+    return GeometryBranches([xy[b, :, 0].tolist() for b in range(4)], [xy[b, :, 1].tolist() for b in range(4)])
+
 # Parameter-dictionary keys and defaults (PyBinaryParams, PYB:103-134).
 _BINARY_PARAM_DEFAULTS = dict(t0=0.0, tE=1.0, u0=0.0, alpha=0.0, s=1.0, q=1.0, q2=0.0, sep2=0.0, ang=0.0, rho=0.0,
                               piEN=0.0, piEE=0.0, g1=0.0, g2=0.0, g3=0.0, lom_szs=0.0, lom_ar=1.0, u0_2=0.0,
@@ -528,6 +565,48 @@ class LightCurve:
 
     def magnification(self, time, params=None, **kw):
         return float(self(np.array([float(time)]), params, **kw)[0])
+
+    _GEOMETRY_KEYWORDS = dict(s=1.0, q=1.0, n_points=1400, time=math.nan, t0=0.0, tE=1.0, u0=0.0, alpha=0.0,
+                              g1=0.0, g2=0.0, g3=0.0, lom_szs=0.0, lom_ar=1.0)
+
+    def _geometry(self, caustic, params, n_points, kw):
+        # caustics_from_dict (PYB:2539-2556) and geometry_branches (PYB:1882-1926).
+        if params is not None:
+            if kw:
+                raise TypeError("pass the parameters either as a dictionary or as keywords")
+            p = dict(_BINARY_PARAM_DEFAULTS)
+            p.update(params)
+            g = dict(self._GEOMETRY_KEYWORDS, s=p["s"], q=p["q"], n_points=1000 if n_points is None else n_points)
+        else:
+            unknown = set(kw) - set(self._GEOMETRY_KEYWORDS)
+            if unknown:
+                raise TypeError(f"unexpected keyword arguments: {sorted(unknown)}")
+            g = dict(self._GEOMETRY_KEYWORDS)
+            g.update(kw)
+            if n_points is not None:
+                g["n_points"] = n_points
+        if int(g["n_points"]) < 8:
+            raise ValueError("n_points must be at least 8")
+        separation = g["s"]
+        if self.orbital_motion_mode != STATIC and math.isfinite(g["time"]):
+            t_ref = self.event.tfix if self.event.tfix != 0.0 else g["t0"]
+            if self.orbital_motion_mode == CIRCULAR:
+                separation = circular_orbital_motion(g["time"], g["s"], g["alpha"], g["g1"], g["g2"], g["g3"],
+                                                     t_ref)[0]
+            else:
+                separation = kepler_orbital_motion(g["time"], g["s"], g["alpha"], g["g1"], g["g2"], g["g3"],
+                                                   g["lom_szs"], g["lom_ar"], t_ref)[0]
+        q = g["q"]
+        q_core = 1.0 / q if (self.options.vbm_compatible and q != 0.0) else q
+        return binary_geometry(separation, q_core, int(g["n_points"]), caustic)
+
+    def caustics(self, params=None, n_points=None, **kw):
+        """LightCurve.caustics (PYB:1525-1542, 2539-2556): four tracked caustic branches."""
+        return self._geometry(True, params, n_points, kw)
+
+    def critical_curves(self, params=None, n_points=None, **kw):
+        """LightCurve.critical_curves (PYB:1544-1561): four tracked critical-curve branches."""
+        return self._geometry(False, params, n_points, kw)
 
     def info(self, times, params=None, **kw):
         """Per-epoch magnifications with the finite-source method chosen."""

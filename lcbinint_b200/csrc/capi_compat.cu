@@ -81,6 +81,7 @@ double wide_binary_offset(double separation, const lcbi_params& p, const lcbi_op
 // arithmetic and C library calls so the values are bit-identical.
 struct Orbit {
     double separation, angle;
+    double line_of_sight = 0.0;
 };
 
 constexpr double kBranchEps = 1.0e-8;
@@ -116,6 +117,7 @@ Orbit circular_orbit(double time, double separation, double angle, double w1, do
     const double sin_angle = (c_phi * s_om + c_inc * s_phi * c_om) / den;
     const double cos_angle = (c_phi * c_om - c_inc * s_phi * s_om) / den;
     o.angle = std::atan2(sin_angle, cos_angle);
+    o.line_of_sight = s_true * std::sin(inc) * s_phi;
     return o;
 }
 
@@ -178,9 +180,11 @@ Orbit kepler_orbit(double time, double separation, double angle, double w1, doub
     const double r1 = semi_major * sqrt0(1.0 - ecc * ecc) * sin_e;
     const double x0 = r0 * x[0] + r1 * y[0];
     const double x1 = r0 * x[1] + r1 * y[1];
+    const double x2 = r0 * x[2] + r1 * y[2];
     Orbit o;
     o.separation = std::sqrt(x0 * x0 + x1 * x1);
     o.angle = angle + std::atan2(x1, x0);
+    o.line_of_sight = x2;
     return o;
 }
 
@@ -519,6 +523,28 @@ lcbi_status lcbi_magnification(double time, const lcbi_params* params, const lcb
 {
     if (params == nullptr || result == nullptr) return LCBI_INVALID_ARGUMENT;
     return lcbi_magnification_array(&time, 1, params, options, result);
+}
+
+int lcbi_circular_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
+                                 double reference_time, double* state)
+{
+    if (!state) return LCBI_INVALID_ARGUMENT;
+    const Orbit o = circular_orbit(time, separation, angle, g1, g2, g3, reference_time);
+    state[0] = o.separation;
+    state[1] = o.angle;
+    state[2] = o.line_of_sight;
+    return LCBI_OK;
+}
+
+int lcbi_kepler_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
+                               double szs, double ar, double reference_time, double* state)
+{
+    if (!state) return LCBI_INVALID_ARGUMENT;
+    const Orbit o = kepler_orbit(time, separation, angle, g1, g2, g3, szs, ar, reference_time);
+    state[0] = o.separation;
+    state[1] = o.angle;
+    state[2] = o.line_of_sight;
+    return LCBI_OK;
 }
 
 const char* lcbi_status_string(lcbi_status status)

@@ -1017,6 +1017,38 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
 
 extern "C" {
 
+int lcbi_gpu_binary_geometry(lcbi_gpu_context* c, double s, double q, int32_t n_points, int32_t caustic,
+                             double* xy, int32_t* points_per_branch)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !xy || n_points < 8) return LCBI_INVALID_ARGUMENT;
+    if (!std::isfinite(s) || !std::isfinite(q) || s == 0.0 || q == 0.0) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    Plan plan;
+    ModelTable mt{&plan};
+    mt.add(s, q, n_points);
+    if (!upload(ctx, ctx->fs_models, plan.models) || !upload(ctx, ctx->fs_raw_offset, plan.raw_offset) ||
+        !upload(ctx, ctx->fs_phases, plan.phases) ||
+        !ctx->ensure(ctx->fs_raw, (4ll * n_points + 1) * sizeof(P2)) ||
+        !ctx->ensure(ctx->fs_branches, (4ll * n_points + 1) * sizeof(P2)))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("geometry", launch_caustics(static_cast<CausticModel*>(ctx->fs_models.ptr), 1, n_points,
+                                                static_cast<double2*>(ctx->fs_phases.ptr),
+                                                static_cast<long long*>(ctx->fs_raw_offset.ptr),
+                                                static_cast<P2*>(ctx->fs_raw.ptr),
+                                                static_cast<P2*>(ctx->fs_branches.ptr), ctx->stream, nullptr,
+                                                caustic == 0)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 2;
+    if (!ctx->check("geometry D2H", cudaMemcpyAsync(xy, ctx->fs_branches.ptr, 4ll * n_points * sizeof(P2),
+                                                    cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    if (points_per_branch) *points_per_branch = n_points;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_last_item_cycles(lcbi_gpu_context* c, int64_t n, int64_t* cycles)
 {
     Context* ctx = reinterpret_cast<Context*>(c);

@@ -28,7 +28,8 @@ __global__ void ld_table_kernel(const double2* __restrict__ coeffs, int n_tables
 __global__ void __launch_bounds__(128) caustic_roots_kernel(const CausticModel* __restrict__ models, int n_models,
                                                            const double2* __restrict__ phases,
                                                            const long long* __restrict__ raw_offset, P2* raw,
-                                                           const unsigned char* __restrict__ needed)
+                                                           const unsigned char* __restrict__ needed,
+                                                           int critical_points)
 {
     // Flattened (model, phase) index; models are laid out back to back.
     const int m = blockIdx.y;
@@ -40,7 +41,8 @@ __global__ void __launch_bounds__(128) caustic_roots_kernel(const CausticModel* 
         critical_roots(md.s, md.q, dc{ph.x, ph.y}, roots);
         P2* out = raw + raw_offset[m] + 4ll * i;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] = lens_equation_complex(md.s, md.q, roots[k]);
+        for (int k = 0; k < 4; ++k)
+            out[k] = critical_points ? P2{roots[k].re, roots[k].im} : lens_equation_complex(md.s, md.q, roots[k]);
     }
 }
 
@@ -202,11 +204,12 @@ cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables
 
 cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,
                             const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream,
-                            const unsigned char* needed)
+                            const unsigned char* needed, bool critical_points)
 {
     if (n_models <= 0) return cudaSuccess;
     dim3 grid((max_bins + 127) / 128, n_models);
-    caustic_roots_kernel<<<grid, 128, 0, stream>>>(models, n_models, phases, raw_offset, raw, needed);
+    caustic_roots_kernel<<<grid, 128, 0, stream>>>(models, n_models, phases, raw_offset, raw, needed,
+                                                   critical_points ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     caustic_track_kernel<<<n_models, 32, 0, stream>>>(models, n_models, raw_offset, raw, branches, needed);

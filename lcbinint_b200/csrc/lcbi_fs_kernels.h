@@ -92,10 +92,12 @@ struct FsWork {
 constexpr int kBigWarps = 8;
 
 cudaError_t launch_ld_tables(const double2* coeffs, int n_tables, double* tables, cudaStream_t stream);
-// needed (optional): models whose flag is 0 are not sampled.
+// needed (optional): models whose flag is 0 are not sampled.  critical_points:
+// track the critical-curve roots themselves (lens frame) instead of their
+// images on the source plane.
 cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, const double2* phases,
                             const long long* raw_offset, P2* raw, P2* branches, cudaStream_t stream,
-                            const unsigned char* needed = nullptr);
+                            const unsigned char* needed = nullptr, bool critical_points = false);
 // Points (rho > 0, finite_mode > 0) whose source is outside the outer caustic
 // box (caustic_outer_box) by the decision's margin get kItemOutsideBox; the
 // others set needed[model_base[i / pass] + model].  needed must be zeroed.

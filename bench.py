@@ -776,6 +776,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N points (small cases for profiler captures)")
+    ap.add_argument("--rays", default="f64", choices=["f64", "f32"],
+                    help="fs_batch: lens map of the inverse-ray cells in FP64 (bit-exact) or FP32 about "
+                         "image-centred anchors (sums FP64); f32 also reports its error against f64")
     ap.add_argument("--models", type=int, default=0,
                     help="orbital workload: use only the first N models (small cases for profiler captures)")
     args = ap.parse_args()
@@ -793,7 +796,9 @@ def main():
         rows = rows[np.random.default_rng(5).permutation(len(rows))[: args.points]]
     config = {"workload": "fs_batch: 4096 forced inverse-ray points, 64 models x 64 epochs, "
                           "Cartesian/polar mixed, nbin 20-200, linear LD",
-              "points": int(len(rows)), "models": 64, "precision": "fp64 (bit-exact vs reference)",
+              "points": int(len(rows)), "models": 64,
+              "precision": "fp64 (bit-exact vs reference)" if args.rays == "f64" else
+                           "fp32 ray map about image-centred anchors, fp64 sums, fp64 seeds and decisions",
               "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
 
     if args.impl == "reference":
@@ -870,6 +875,12 @@ def main():
                                    res_host.ctypes.data, 0)
         ctx.check(rc, "lcbi_gpu_binary_mag")
 
+    fp32_error = None
+    if args.rays == "f32":
+        # The FP64 magnifications of the same points, for the FP32 arm's error.
+        step_device()
+        res64 = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=FS_RESULT_DTYPE)["magnification"].copy()
+        L.lcbi_gpu_set_ray_precision(ctx.handle, 32)
     for _ in range(args.warmup):
         flush_l2(flush)
         step_device()
@@ -900,6 +911,13 @@ def main():
     rays = np.zeros(n, dtype=np.uint64)
     L.lcbi_gpu_last_ray_counts(ctx.handle, n, _lib.ptr(rays))
     res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=FS_RESULT_DTYPE)
+    if args.rays == "f32":
+        a32 = res["magnification"]
+        ok = np.isfinite(a32) & np.isfinite(res64) & (res64 != 0)
+        rel = np.abs(a32[ok] / res64[ok] - 1.0)
+        fp32_error = {"vs": "the same points with the FP64 map (bit-exact with the reference)",
+                      "points": int(ok.sum()), "max_rel": float(rel.max()), "p99_rel": float(np.quantile(rel, 0.99)),
+                      "median_rel": float(np.median(rel)), "identical": int((rel == 0).sum())}
 
     # end to end: host arrays through the public C ABI (planning, H2D copies,
     # kernels, D2H of the results), wall-clocked per step
@@ -951,6 +969,8 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    if fp32_error is not None:
+        out["fp32_error"] = fp32_error
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         rate, nn, wall = cpu_reference_rate(rows, ncores, target_seconds=args.cpu_seconds)
         out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",

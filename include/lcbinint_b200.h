@@ -68,6 +68,18 @@ int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles)
  * a block) for calls of at most 4 points per SM until this is called.  Results
  * are the same for every value. */
 int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
+/* Precision of the inverse-ray lens map (no reference counterpart; the
+ * reference maps every cell in FP64).  64 (the default): the reference's FP64
+ * map, bit-exact.  32: each Cartesian scan maps its cells in FP32 about its
+ * seed, and each polar tile column about its middle radius -- the map at the
+ * anchor in FP64 plus the difference to the cell in FP32, so the rounding is
+ * relative to the cell's offset from the anchor -- while every sum stays
+ * FP64.  Cells within about 1e-7 rho of the source's limb can change sides, so
+ * magnifications differ from the FP64 ones by ~1e-7 relative, the limb-darkening
+ * table index by a few 1e-3 of a step.  Seeds, decisions and the start cells
+ * stay FP64. */
+int lcbi_gpu_set_ray_precision(lcbi_gpu_context *ctx, int32_t bits);
+
 /* Polar inverse ray in the first pass: 1 (default) the tile-parallel flood
  * fill spread over the whole GPU, 0 the one-warp-per-point segment flood fill.
  * Both count the same cells; results are the same.  No reference counterpart. */

@@ -221,6 +221,14 @@ int lcbi_gpu_set_cell_budget(lcbi_gpu_context* c, int64_t cells)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_ray_precision(lcbi_gpu_context* c, int32_t bits)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || (bits != 32 && bits != 64)) return LCBI_INVALID_ARGUMENT;
+    ctx->f32_rays = bits == 32;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_set_polar_tiles(lcbi_gpu_context* c, int enable)
 {
     Context* ctx = reinterpret_cast<Context*>(c);

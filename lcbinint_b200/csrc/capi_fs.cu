@@ -270,6 +270,7 @@ FsWork common_work(Context* ctx)
     // sources) run every point on a whole block.
     w.cell_budget = ctx->cell_budget;
     w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
+    w.f32_rays = ctx->f32_rays ? 1 : 0;
     return w;
 }
 

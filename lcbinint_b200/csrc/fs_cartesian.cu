@@ -127,6 +127,8 @@ struct Ctx {
     bool uniform;
     const double* ld;
     int max_steps;
+    bool f32;                 // FP32 map about the current seed (A)
+    Anchor32 A;
 };
 
 // Lens map of one cell, as the reference evaluates it for the current scan.
@@ -134,7 +136,14 @@ __device__ __forceinline__ void eval_for_scan(const Ctx& C, double x, double y, 
 {
     double md2;
     bool ok = true;
-    if (jsign == 0) {
+    if (C.f32) {
+        md2 = static_cast<double>(anchored_dist2(C.A, x, y));
+        if (jsign != 0) {
+            const float j = anchored_jacobian(C.A, x, y);
+            const int es = j > 0.0f ? 1 : (j < 0.0f ? -1 : 0);
+            ok = es != -jsign;
+        }
+    } else if (jsign == 0) {
         md2 = mapped_dist2(C.m, x, y, C.src);
     } else {
         double jac;
@@ -575,6 +584,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
             C.bulk = C.uniform || (st.ld_c >= 0.0 && st.ld_d >= 0.0 && st.ld_c + st.ld_d < 1.0);
             C.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
             C.max_steps = max(100000, st.source_bins * st.source_bins * 2000);
+            C.f32 = w.f32_rays != 0;
             const double nbin = static_cast<double>(max(st.source_bins, 1));
             const double incr = rho / nbin;
             const double margin = 0.5 * incr * 1.01;
@@ -593,6 +603,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
                 R.ovf = false;
                 rows_ensure<W>(R, 1);
                 const P2 seed = seeds[ii];
+                if (C.f32) C.A = make_anchor32(C.m, seed.x, seed.y, C.src);
                 double areai = 0.0;
                 double dy = incr;
                 int yi = 0;

@@ -55,7 +55,7 @@ struct TileItem {
     int phi_bins;
     int uniform;
     int state;
-    int pad;
+    int f32;                 // cells mapped in FP32 about a per-column anchor
     unsigned long long acc_lo;
     long long acc_hi;
     unsigned long long cells;
@@ -182,6 +182,14 @@ __device__ __forceinline__ double cell_dz2(const TileItem& I, double cs, double 
     return dist2(mp, I.src);
 }
 
+// As cell_dz2, in FP32 about the anchor A when the item asks for FP32 rays.
+__device__ __forceinline__ double cell_dz2_rays(const TileItem& I, const Anchor32& A, double cs, double sn, int ir)
+{
+    if (!I.f32) return cell_dz2(I, cs, sn, ir);
+    const double radius = (static_cast<double>(ir) + 0.5) * I.dr;
+    return static_cast<double>(anchored_dist2(A, radius * cs, radius * sn));
+}
+
 // One visit of one tile by one warp.
 __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
 {
@@ -204,6 +212,12 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
         const double phi = (static_cast<double>(g) + 0.5) * I.dphi;
         sincos(phi, &sn, &cs);
     }
+    // FP32 rays: one anchor per lattice column of the tile, at its middle radius.
+    Anchor32 A{};
+    if (I.f32 && valid) {
+        const double ra = (static_cast<double>(tr * 32) + 16.0) * I.dr;
+        A = make_anchor32(I.m, ra * cs, ra * sn, I.src);
+    }
     int ready = 0;
     if (j == 0) ready = ld_cg_i32(&T->mready);
     ready = __shfl_sync(kFull, ready, 0);
@@ -214,7 +228,7 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
             const int base = tr * 32;
 #pragma unroll 4
             for (int c = 0; c < 32; ++c) {
-                const double d2 = cell_dz2(I, cs, sn, base + c);
+                const double d2 = cell_dz2_rays(I, A, cs, sn, base + c);
                 d2s[c * 32 + j] = d2;
                 if (d2 <= I.rho2) M |= 1u << c;
             }
@@ -252,7 +266,7 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
         const double radius = (static_cast<double>(ir) + 0.5) * I.dr;
         double b = 1.0;
         if (!I.uniform) {
-            const double d2 = fresh ? d2s[c * 32 + j] : cell_dz2(I, cs, sn, ir);
+            const double d2 = fresh ? d2s[c * 32 + j] : cell_dz2_rays(I, A, cs, sn, ir);
             b = ld_lookup(I.ld, d2 * I.inv_rho2);
         }
         fx_add_double(acc, b * radius);
@@ -368,6 +382,7 @@ __global__ void __launch_bounds__(128) tile_start_kernel(FsWork w, TileCtx G)
         I.inv_rho2 = 1.0 / I.rho2;
         I.uniform = (st.ld_c == 0.0 && st.ld_d == 0.0) ? 1 : 0;
         I.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
+        I.f32 = w.f32_rays;
         if (isfinite(I.flux)) I.state = (I.phi_bins >= (1 << 30)) ? kTileOverflow : kTileActive;
     }
     if (lane_id() == 0) G.items[k] = I;

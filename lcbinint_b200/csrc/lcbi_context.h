@@ -63,6 +63,7 @@ struct Context {
     bool big_ready = false;
     // Tile-parallel polar flood fill: table and FIFO capacity (power of two).
     bool polar_tiles = true;
+    bool f32_rays = false;     // inverse-ray cells mapped in FP32 about image-centred anchors
     long long tile_capacity = 1 << 20;
     int tile_blocks = 0;       // persistent flood blocks (0: occupancy x SMs)
     // Adjoint: cells per source radius of the gradient lattice, flood blocks.

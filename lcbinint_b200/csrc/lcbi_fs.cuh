@@ -79,6 +79,70 @@ __device__ __forceinline__ double mapped_dist2(const Mapper& m, double x, double
     return dx * dx + dy * dy;
 }
 
+// FP32 ray map about an image-centred anchor Z (FP64): the map of a cell
+// z = Z + d is the FP64 map at Z plus a difference formed in FP32,
+//   w(Z + d) - w(Z) = d + m1 conj(d / (U1 (U1 + d))) + m2 conj(d / (U2 (U2 + d))),
+// U1 = Z - a, U2 = Z (from 1/conj(U + d) - 1/conj(U) = -conj(d / (U (U + d)))),
+// so the FP32 rounding is relative to the cell's offset from the anchor, not
+// to its position, and the squared distance to the source is accumulated
+// from the anchor's FP64 offset.  Used only when a context asks for FP32 rays.
+struct Anchor32 {
+    double zx, zy;           // anchor
+    float wx, wy;            // map(anchor) - source
+    float u1x, u1y, u2x, u2y;
+    float m1, m2;
+};
+
+__device__ __forceinline__ Anchor32 make_anchor32(const Mapper& m, double zx, double zy, P2 src)
+{
+    Anchor32 A;
+    A.zx = zx;
+    A.zy = zy;
+    const P2 w = map_real(m, zx, zy);
+    A.wx = static_cast<float>(w.x - src.x);
+    A.wy = static_cast<float>(w.y - src.y);
+    A.u1x = static_cast<float>(zx - m.a);
+    A.u1y = static_cast<float>(zy);
+    A.u2x = static_cast<float>(zx);
+    A.u2y = static_cast<float>(zy);
+    A.m1 = static_cast<float>(m.m1);
+    A.m2 = static_cast<float>(m.m2);
+    return A;
+}
+
+// m conj(d / (U (U + d))) for one lens.
+__device__ __forceinline__ void anchor_term(float ux, float uy, float m, float dx, float dy, float* tx, float* ty)
+{
+    const float vx = ux + dx, vy = uy + dy;
+    const float px = ux * vx - uy * vy, py = ux * vy + uy * vx;
+    const float f = m / (px * px + py * py);
+    *tx = (dx * px + dy * py) * f;
+    *ty = (dx * py - dy * px) * f;
+}
+
+__device__ __forceinline__ float anchored_dist2(const Anchor32& A, double x, double y)
+{
+    const float dx = static_cast<float>(x - A.zx), dy = static_cast<float>(y - A.zy);
+    float t1x, t1y, t2x, t2y;
+    anchor_term(A.u1x, A.u1y, A.m1, dx, dy, &t1x, &t1y);
+    anchor_term(A.u2x, A.u2y, A.m2, dx, dy, &t2x, &t2y);
+    const float ex = A.wx + (dx + t1x + t2x);
+    const float ey = A.wy + (dy + t1y + t2y);
+    return ex * ex + ey * ey;
+}
+
+// Jacobian determinant 1 - |m1/u1^2 + m2/u2^2|^2 of the cell, in FP32.
+__device__ __forceinline__ float anchored_jacobian(const Anchor32& A, double x, double y)
+{
+    const float dx = static_cast<float>(x - A.zx), dy = static_cast<float>(y - A.zy);
+    const float ax = A.u1x + dx, ay = A.u1y + dy, bx = A.u2x + dx, by = A.u2y + dy;
+    const float ia = 1.0f / (ax * ax + ay * ay), ib = 1.0f / (bx * bx + by * by);
+    // m / u^2 = m conj(u)^2 / |u|^4
+    const float re = A.m1 * (ax * ax - ay * ay) * ia * ia + A.m2 * (bx * bx - by * by) * ib * ib;
+    const float im = -2.0f * (A.m1 * ax * ay * ia * ia + A.m2 * bx * by * ib * ib);
+    return 1.0f - (re * re + im * im);
+}
+
 // evaluate_binary_lens_cell (FSM:121-153): distance and Jacobian sharing denominators.
 __device__ __forceinline__ double eval_cell(const Mapper& m, double x, double y, P2 src, double* jac)
 {

@@ -87,6 +87,9 @@ struct FsWork {
     // First pass only: when a list holds at most this many points (0: never),
     // the budget is one cell, so every point of the list runs on a block.
     int few_points;
+    // Inverse-ray cells mapped in FP32 about an image-centred anchor (sums
+    // stay FP64); 0: the reference's FP64 map, bit-exact.
+    int f32_rays;
 };
 
 constexpr int kBigWarps = 8;

@@ -310,11 +310,13 @@ int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context *ctx, const lcbi_fs_settings *s
  * library unchanged.  The magnification runs on the calling thread's current
  * CUDA device, through a context kept per host thread.  Built: binary lenses
  * (q2 <= 0, no parallax, no xallarap), static or with circular or Keplerian
- * lens orbital motion (src/lcbinint/model/orbital_motion.cpp:69-206), in both
- * coordinate conventions, point and finite source, bit-identical to the
- * reference.  Parameter sets that need the rest (triple lenses, parallax,
- * xallarap) return LCBI_UNSUPPORTED, with the result filled as the reference
- * fills it for unsupported input (NaN magnifications, the source position). */
+ * lens orbital motion (src/lcbinint/model/orbital_motion.cpp:69-206),
+ * annual and terrestrial parallax and xallarap
+ * (src/lcbinint/model/trajectory.cpp:185-463; see lcbi_set_earth_ephemeris),
+ * in both coordinate conventions, point and finite source, bit-identical to
+ * the reference.  Triple lenses return LCBI_UNSUPPORTED, with the result
+ * filled as the reference fills unsupported input (NaN magnifications, the
+ * source position). */
 #ifndef LCBININT_H
 typedef enum lcbi_orbital_motion_mode {
     LCBI_ORBIT_STATIC = 0,
@@ -445,6 +447,17 @@ int lcbi_circular_orbital_motion(double time, double separation, double angle, d
                                  double reference_time, double *state);
 int lcbi_kepler_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
                                double szs, double ar, double reference_time, double *state);
+
+/* The Earth ephemeris for annual parallax (no counterpart in the reference's
+ * ABI: the reference reads the file named by the LCBININT_EARTH_EPHEMERIS
+ * environment variable, else its compiled-in data/earth_orbital_parallax_table.txt,
+ * once per process; src/lcbinint/model/trajectory.cpp:128-183).  This library
+ * reads the same environment variable on first use; this call loads a JPL
+ * Horizons vector table (JD, x, y, z, vx, vy, vz in AU and AU/day, between
+ * $$SOE and $$EOE) explicitly instead.  Returns the number of states read, or
+ * -1 if the file cannot be opened.  Without a table every parallax epoch is a
+ * numerical error, as in the reference. */
+int lcbi_set_earth_ephemeris(const char *path);
 
 #define LCBI_ARRAYS_KEYWORD_ROUTE 1u
 int lcbi_gpu_magnification_arrays(lcbi_gpu_context *ctx, int32_t n_sets, const lcbi_params *params,

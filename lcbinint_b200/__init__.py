@@ -14,7 +14,7 @@ from ._lib import GpuError, LibraryMissing, context
 from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, GeometryBranches, LightCurve, LightCurveFunc,
                   LightCurveInfo, LimbDarkening, Options, binary_geometry, binary_inverse_ray,
                   binary_inverse_ray_batch, binary_mag, circular_orbital_motion, kepler_orbital_motion, light_curves,
-                  magnification_arrays)
+                  magnification_arrays, set_earth_ephemeris)
 
 __all__ = [
     "binary_mag0",
@@ -28,6 +28,7 @@ __all__ = [
     "GeometryBranches",
     "circular_orbital_motion",
     "kepler_orbital_motion",
+    "set_earth_ephemeris",
     "LightCurve",
     "LightCurveFunc",
     "LightCurveInfo",

@@ -355,6 +355,16 @@ CIRCULAR = 1
 KEPLER = 2
 
 
+def set_earth_ephemeris(path) -> int:
+    """Loads the Earth ephemeris for annual parallax (a JPL Horizons vector
+    table) instead of the file named by LCBININT_EARTH_EPHEMERIS; returns the
+    number of states read (lcbi_set_earth_ephemeris)."""
+    n = _lib.lib().lcbi_set_earth_ephemeris(str(path).encode())
+    if n < 0:
+        raise FileNotFoundError(str(path))
+    return n
+
+
 def circular_orbital_motion(time, separation, angle, g1=0.0, g2=0.0, g3=0.0, reference_time=0.0):
     """lcbinint.circular_orbital_motion (PYB:3896-3908): (separation, angle,
     line-of-sight separation) of a circular lens orbit at `time`."""
@@ -475,14 +485,15 @@ class LightCurve:
 
     Routes as the reference does.  The static binary lens in VBM coordinates
     takes the direct fast path (PYB:1087-1174, lcbi_gpu_light_curves).  Lens
-    orbital motion (circular or Keplerian) and the original / centre-of-mass
-    conventions take LensModel's path when the parameters come as a
-    dictionary (PYB:2325-2358 -> lens_model.cpp) and the dynamic path when
-    they come as keywords (PYB:1364-1385, 1958-2060); both run through
-    lcbi_gpu_magnification_arrays.  Binary sources blend two single-source
-    curves (PYB:2331-2354).  Parallax needs the reference's Earth ephemeris
-    and triple lenses are outside this implementation: both raise
-    NotImplementedError."""
+    orbital motion (circular or Keplerian), annual and terrestrial parallax
+    (with an Earth ephemeris: set_earth_ephemeris or the
+    LCBININT_EARTH_EPHEMERIS environment variable), xallarap and the
+    original / centre-of-mass conventions take LensModel's path when the
+    parameters come as a dictionary (PYB:2325-2358 -> lens_model.cpp) and the
+    dynamic path when they come as keywords (PYB:1364-1385, 1958-2060); both
+    run through lcbi_gpu_magnification_arrays.  Binary sources blend two
+    single-source curves (PYB:2331-2354).  Triple lenses are outside this
+    implementation and raise NotImplementedError."""
 
     _KEYWORDS = ("t0", "tE", "u0", "alpha", "s", "q", "rho", "piEN", "piEE", "g1", "g2", "g3", "lom_szs", "lom_ar")
 
@@ -499,8 +510,6 @@ class LightCurve:
             source = "binary"
         else:
             raise ValueError("source must be 'single' or 'binary'")
-        if parallax or terrestrial_parallax:
-            raise NotImplementedError("parallax needs the reference's Earth ephemeris table, which is not available")
         self.lens = "binary_lens"
         self.source = source
         self.event = event or EventCoordinates()
@@ -512,22 +521,32 @@ class LightCurve:
         self.parallax = parallax
         self.terrestrial_parallax = terrestrial_parallax
 
-    def _direct(self, p=None) -> bool:
+    def _direct(self, p=None, keyword_route=False) -> bool:
         # can_use_direct_static_binary (PYB:494-503); for dictionaries also
         # evaluate_binary_light_curve_numpy's test (PYB:1105-1118).
         o = self.options
         if not (self.orbital_motion_mode == STATIC and o.vbm_compatible and not o.center_of_mass):
             return False
-        if p is not None:
-            return all(p.get(k, 0.0) == 0.0 for k in ("xi_1", "xi_2", "piEN_xa", "piEE_xa"))
-        return True
+        if keyword_route:
+            # The keyword overloads take the dynamic path whenever the curve
+            # has parallax (PYB:2360-2405).
+            return not self.parallax
+        keys = ("xi_1", "xi_2", "piEN_xa", "piEE_xa") + (("piEN", "piEE") if self.parallax else ())
+        return all(p.get(k, 0.0) == 0.0 for k in keys)
 
     def _single(self, times, p, keyword_route=False):
-        if self._direct(None if keyword_route else p):
+        if self._direct(p, keyword_route):
             (A,), (m,), (st,) = light_curves([times], [p], self.options, self.limb_darkening, return_method=True)
             _raise_for_status(st)
             return A
-        cp = binary_c_params([p], self.limb_darkening, self.event, self.orbital_motion_mode)
+        if keyword_route:
+            # PyLightCurveFunc::dynamic_light_curve (PYB:1364-1385): parallax
+            # components as given, the observatory from the event coordinates.
+            cp = binary_c_params([p], self.limb_darkening, self.event, self.orbital_motion_mode, parallax=True,
+                                 terrestrial_parallax=True)
+        else:
+            cp = binary_c_params([p], self.limb_darkening, self.event, self.orbital_motion_mode,
+                                 parallax=self.parallax, terrestrial_parallax=self.terrestrial_parallax)
         (res,), status = magnification_arrays([times], cp, self.options, keyword_route=keyword_route)
         _raise_for_c_status(status)
         return res["magnification"].copy()
@@ -545,6 +564,8 @@ class LightCurve:
             unknown = set(kw) - set(self._KEYWORDS)
             if unknown:
                 raise TypeError(f"unexpected keyword arguments: {sorted(unknown)}")
+            if ("piEN" in kw or "piEE" in kw) and not self.parallax:
+                raise ValueError("piEN/piEE require LightCurve(parallax=True); the current trajectory model is static")
             p = dict(kw)
             keyword_route = True
         if self.source == "binary":

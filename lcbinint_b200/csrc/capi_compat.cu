@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "lcbi_internal.h"
+#include "lcbi_trajectory.h"
 
 namespace {
 
@@ -282,9 +283,10 @@ void prepare_set(const lcbi_params& p, const lcbi_options& o, bool keyword_route
                               (o.xallarap_param_type == LCBI_XALLARAP_ANGULAR_VELOCITY
                                    ? (p.xi_1 != 0.0 || p.xi_2 != 0.0)
                                    : (p.piEN_xa != 0.0 || p.piEE_xa != 0.0));
-    if (p.piEN != 0.0 || p.piEE != 0.0 || has_xallarap || p.q2 > 0.0) {
-        // Parallax, xallarap and triple lenses are not built here: the first
-        // epoch is reported as unsupported.
+    const bool parallax = p.piEN != 0.0 || p.piEE != 0.0;
+    if (p.q2 > 0.0) {
+        // Triple lenses are not built here: the first epoch is reported as
+        // unsupported.
         const double nan = std::numeric_limits<double>::quiet_NaN();
         info.status = LCBI_UNSUPPORTED;
         info.write_first = true;
@@ -299,10 +301,15 @@ void prepare_set(const lcbi_params& p, const lcbi_options& o, bool keyword_route
     const double eff_q = (vbm && p.q != 0.0) ? 1.0 / p.q : p.q;
     const double rho = std::abs(p.rho);
     long long n_valid = n;
+    // Parallax or xallarap: Trajectory::source_position (trajectory.cpp:436-463).
+    const bool dynamic_source = parallax || has_xallarap;
+    const lcbi::Trajectory traj = dynamic_source ? lcbi::make_trajectory(p) : lcbi::Trajectory{};
     for (long long i = 0; i < n; ++i) {
         const double tn = (times[i] - p.t0) / p.tE;
         double x, y;
-        if (vbm) {
+        if (dynamic_source) {
+            lcbi::source_position(traj, times[i], vbm, o.xallarap_param_type, &x, &y);
+        } else if (vbm) {
             x = tn * cos_t - beta * sin_t;
             y = tn * sin_t + beta * cos_t;
         } else {
@@ -310,7 +317,10 @@ void prepare_set(const lcbi_params& p, const lcbi_options& o, bool keyword_route
             y = beta * cos_t - tn * sin_t;
         }
         const Orbit orb = static_orbit ? Orbit{p.sep, p.theta} : orbit_at(p, times[i]);
-        if (!std::isfinite(orb.separation) || !std::isfinite(orb.angle)) {
+        if (!std::isfinite(orb.separation) || !std::isfinite(orb.angle) || !std::isfinite(x) ||
+            !std::isfinite(y)) {
+            // A non-finite orbit ends the array (lens_model.cpp:116-119); so
+            // does a source outside the ephemeris, whose magnification is NaN.
             n_valid = i;
             info.bad_x = x;
             info.bad_y = y;
@@ -318,10 +328,11 @@ void prepare_set(const lcbi_params& p, const lcbi_options& o, bool keyword_route
         }
         if (!static_orbit) {
             if (vbm) {
-                // LensModel rotates (tau, beta) directly; the keyword route
-                // first takes them back out of the trajectory point.
+                // LensModel rotates (tau, beta) directly unless parallax moved
+                // the source (lens_model.cpp:164-178); the keyword route always
+                // takes them back out of the trajectory point.
                 double tau = tn, b = beta;
-                if (keyword_route) {
+                if (keyword_route || parallax) {
                     tau = x * cos_t + y * sin_t;
                     b = -x * sin_t + y * cos_t;
                 }

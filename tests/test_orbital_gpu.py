@@ -119,12 +119,12 @@ def test_batched_sets_match_single_calls():
 
 def test_status_per_set():
     """Per-set statuses as lcbi_magnification_array reports them: an invalid
-    set, an unsupported one (parallax) and a good one in one batch."""
+    set, an unsupported one (a triple lens) and a good one in one batch."""
     rng = np.random.default_rng(340)
     good = _model(rng, api.CIRCULAR)
     cps = api.binary_c_params([good, good, good], orbital_motion_mode=api.CIRCULAR)
     cps[0]["tE"] = 0.0
-    cps[1]["piEN"] = 0.2
+    cps[1]["q2"] = 0.2
     times = [np.linspace(-10, 10, 5)] * 3
     res, status = api.magnification_arrays(times, cps)
     assert list(status) == [1, 3, 0]

@@ -207,12 +207,14 @@ def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
     order = rng.permutation(len(rows))
     ctx = mp.get_context("spawn")
     with ctx.Pool(n_procs) as pool:
-        # calibrate on one point per process
-        take = order[:n_procs]
+        # warm the workers up (imports, library loads), then calibrate on four
+        # points per process
+        pool.map(_ref_worker, [([rows[i]],) for i in order[:n_procs]])
+        take = order[n_procs:5 * n_procs]
         t0 = time.perf_counter()
-        pool.map(_ref_worker, [([rows[i]],) for i in take])
+        pool.map(_ref_worker, [([rows[i] for i in take[k::n_procs]],) for k in range(n_procs)])
         cal = time.perf_counter() - t0
-        per_point = max(cal, 1e-3)  # one point per process in parallel
+        per_point = max(cal / 4.0, 1e-4)  # per point, per process, in parallel
         m = int(max(1, min(len(rows) // n_procs, target_seconds / per_point)))
         sample = order[: m * n_procs]
         chunks = [([rows[i] for i in sample[k::n_procs]],) for k in range(n_procs)]
@@ -284,14 +286,14 @@ def cpu_adjoint_rate(P, T, n_procs, n_models):
     return n / wall / 17.0, n, wall
 
 
-def orbital_workload(seed=3, n_models=1024, n_epochs=2000):
+def orbital_workload(seed=3, n_models=1024, n_epochs=2000, parallax=False):
     """Config 5, its lens-orbital-motion half: models drawn as in config 3
     (t0 U[-20, 20] d, tE U[10, 40] d), half of them on circular and half on
     Keplerian orbits with ds/dt / s and dalpha/dt U[-1, 1] per year and the
     line-of-sight term g3 U[0, 0.5] per year (Keplerian: lom_szs U[-0.5, 0.5],
-    lom_ar U[1, 2]); 2000 epochs spanning 200 days.  Returns the parameter
-    dictionaries, their orbital-motion modes, their limb-darkening
-    coefficients and the epochs."""
+    lom_ar U[1, 2]); 2000 epochs spanning 200 days; with parallax, piEN and
+    piEE U[-0.5, 0.5].  Returns the parameter dictionaries, their
+    orbital-motion modes, their limb-darkening coefficients and the epochs."""
     rng = np.random.default_rng(seed)
     dicts, modes, gams = [], [], []
     for m in range(n_models):
@@ -307,7 +309,30 @@ def orbital_workload(seed=3, n_models=1024, n_epochs=2000):
         dicts.append(p)
         modes.append(mode)
         gams.append(float(rng.uniform(0.0, 0.8)))
+    if parallax:
+        # Drawn from a stream of their own, so that the rest of the workload is
+        # the same with and without parallax.
+        prng = np.random.default_rng(seed + 1000)
+        for p in dicts:
+            p.update(piEN=float(prng.uniform(-0.5, 0.5)), piEE=float(prng.uniform(-0.5, 0.5)))
     return dicts, modes, gams, np.linspace(-100.0, 100.0, n_epochs)
+
+
+# Sky position of the config-5 events (the Galactic bulge) for parallax.
+ORBITAL_EVENT = dict(ra=268.5, dec=-29.0)
+
+
+def orbital_ephemeris():
+    """A synthetic Earth ephemeris for the parallax half of config 5 (the
+    reference's table is not in its repository), named through
+    LCBININT_EARTH_EPHEMERIS so that this process, the reference and the CPU
+    workers read the same one."""
+    import tempfile
+    from lcbinint_b200.ephemeris import write_synthetic_ephemeris
+    path = os.path.join(tempfile.mkdtemp(prefix="lcbi_eph_"), "earth.txt")
+    write_synthetic_ephemeris(path)
+    os.environ["LCBININT_EARTH_EPHEMERIS"] = path
+    return path
 
 
 def _ref_orbital_worker(args):
@@ -321,7 +346,9 @@ def _ref_orbital_worker(args):
     t = time.perf_counter()
     n = 0
     for p, mode, gam, times in tasks:
-        lc = ref.LightCurve(limb_darkening=ref.LimbDarkening.linear(gam), orbital_motion_mode=modes[mode])
+        par = "piEN" in p
+        lc = ref.LightCurve(limb_darkening=ref.LimbDarkening.linear(gam), orbital_motion_mode=modes[mode],
+                            parallax=par, event=ref.EventCoordinates(**ORBITAL_EVENT))
         lc(times, p)
         n += len(times)
     return time.perf_counter() - t, n
@@ -648,19 +675,24 @@ def run_adjoint(args, world, rank, local_rank, ncores, common):
 
 
 def run_orbital(args, world, rank, local_rank, ncores, common):
-    """Config 5, lens-orbital-motion half: 1024 models x 2000 epochs with
-    circular or Keplerian lens orbital motion through the batched C ABI
+    """Config 5: 1024 models x 2000 epochs with circular or Keplerian lens
+    orbital motion and annual parallax through the batched C ABI
     (lcbi_gpu_magnification_arrays, LensModel's route), host arrays in and
-    out.  The parallax half needs the reference's Earth ephemeris table,
-    which is missing, so parallax is not applied."""
-    dicts, modes, gams, times = orbital_workload(seed=3 + rank)
+    out.  The Earth ephemeris is synthetic (the reference's table is not in
+    its repository); --no-parallax measures the orbital-motion half alone."""
+    parallax = not args.no_parallax
+    if parallax:
+        orbital_ephemeris()
+    dicts, modes, gams, times = orbital_workload(seed=3 + rank, parallax=parallax)
     if args.models > 0:
         dicts, modes, gams = dicts[:args.models], modes[:args.models], gams[:args.models]
     M, K = len(dicts), times.size
     n = M * K
     config = {"workload": f"orbital: {M} models x 2000 epochs over 200 days, half circular / half Keplerian lens "
                           "orbital motion (g1, g2 U[-1,1]/yr, g3 U[0,0.5]/yr), config-3 model distribution, "
-                          "linear LD U[0,0.8], auto decision tree, nbin 50; parallax not applied (no ephemeris)",
+                          "linear LD U[0,0.8], auto decision tree, nbin 50; " +
+                          ("annual parallax piEN, piEE U[-0.5,0.5] (synthetic Earth ephemeris, event at the "
+                           "Galactic bulge)" if parallax else "no parallax"),
               "points": n, "l2": "not flushed (per-epoch caustic samples, 2.9 GB per chunk, exceed L2)",
               "parallelism": f"replicas x{world}"}
     if args.impl == "reference":
@@ -686,7 +718,9 @@ def run_orbital(args, world, rank, local_rank, ncores, common):
     from lcbinint_b200 import _lib, api
     ctx = lb.context(local_rank)
     L = ctx._L
-    cps = np.concatenate([api.binary_c_params([p], lb.LimbDarkening.linear(g), orbital_motion_mode=m)
+    ev = lb.EventCoordinates(**ORBITAL_EVENT)
+    cps = np.concatenate([api.binary_c_params([p], lb.LimbDarkening.linear(g), ev, orbital_motion_mode=m,
+                                              parallax=parallax)
                           for p, m, g in zip(dicts, modes, gams)])
     co = lb.Options().c_options()
     first = (np.arange(M, dtype=np.int64) * K)
@@ -779,6 +813,8 @@ def main():
     ap.add_argument("--rays", default="f64", choices=["f64", "f32"],
                     help="fs_batch: lens map of the inverse-ray cells in FP64 (bit-exact) or FP32 about "
                          "image-centred anchors (sums FP64); f32 also reports its error against f64")
+    ap.add_argument("--no-parallax", action="store_true",
+                    help="orbital workload: lens orbital motion only (no annual parallax)")
     ap.add_argument("--models", type=int, default=0,
                     help="orbital workload: use only the first N models (small cases for profiler captures)")
     args = ap.parse_args()

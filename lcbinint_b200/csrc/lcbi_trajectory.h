@@ -29,6 +29,7 @@ const std::vector<EarthState>& earth_ephemeris();
 // (the reference caches it per thread for the same sky position and time).
 struct Trajectory {
     lcbi_params p{};
+    const std::vector<EarthState>* eph = nullptr;  // the ephemeris, fetched once per set
     bool annual = false;
     double time_offset = 0.0, eph_reference_time = 0.0;
     std::array<double, 3> north{}, east{}, event{};

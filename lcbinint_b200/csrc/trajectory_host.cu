@@ -117,9 +117,8 @@ std::vector<EarthState> g_eph;
 // interpolate_earth_state (trajectory.cpp:185-207): linear between the
 // bracketing states, NaN outside the table.  A time equal to the last state's
 // reads the last interval.
-void interpolate(double time, V3* pos, V3* vel)
+void interpolate(const std::vector<EarthState>& st, double time, V3* pos, V3* vel)
 {
-    const auto& st = earth_ephemeris();
     if (st.size() < 2 || time < st.front().time || time > st.back().time) {
         const double nan = std::numeric_limits<double>::quiet_NaN();
         *pos = {nan, nan, nan};
@@ -150,7 +149,7 @@ double emit_time(const Trajectory& tr, double observation_time)
     double emit = observation_time;
     for (int i = 0; i < 5; ++i) {
         V3 pos, vel;
-        interpolate(emit, &pos, &vel);
+        interpolate(*tr.eph, emit, &pos, &vel);
         const double light = dot3(pos, tr.event) * kAuLightTravelDays;
         emit = observation_time - light;
     }
@@ -160,7 +159,7 @@ double emit_time(const Trajectory& tr, double observation_time)
 void projected(const Trajectory& tr, double time, double* pn, double* pe, double* vn, double* ve)
 {
     V3 pos, vel;
-    interpolate(time, &pos, &vel);
+    interpolate(*tr.eph, time, &pos, &vel);
     *pn = -dot3(pos, tr.north);
     *pe = -dot3(pos, tr.east);
     *vn = -dot3(vel, tr.north);
@@ -221,6 +220,7 @@ Trajectory make_trajectory(const lcbi_params& p)
 {
     Trajectory tr;
     tr.p = p;
+    tr.eph = &earth_ephemeris();
     tr.annual = p.piEN != 0.0 || p.piEE != 0.0;
     if (tr.annual) {
         const double reference_time = p.tfix != 0.0 ? p.tfix : p.t0;

@@ -144,8 +144,9 @@ typedef struct lcbi_fs_settings {
     double adaptive_hex_threshold;   /* hexadecapole tolerance */
     double limb_darkening_c;
     double limb_darkening_d;
-    int32_t adaptive_source_bins;    /* must be 0: local adaptive refinement is not implemented */
-    int32_t max_source_bins;
+    int32_t adaptive_source_bins;    /* nonzero with a tolerance below: local adaptive refinement
+                                        (finite_source_magnifier.cpp:3074-3289) of Cartesian points */
+    int32_t max_source_bins;         /* below 4096 when refining (the tape holds at most 4096 cells) */
     double finite_source_tol;
     double finite_source_reltol;
 } lcbi_fs_settings;
@@ -190,6 +191,11 @@ typedef struct lcbi_fs_result {
 #define LCBI_GPU_LIMIT_SEEDS 17
 #define LCBI_GPU_LIMIT_ROWS 18
 #define LCBI_GPU_LIMIT_QUEUE 19
+/* Adaptive refinement of a point that the reference would first scan again
+ * at twice the bins (needs_global_topology_retry, finite_source_magnifier.cpp:
+ * 1108-1121: fewer than 50 bins, at least 16 seeds, 100 overlaps, 1,000 gap
+ * repairs and a 1,000-cell jump): that rerun is not built. */
+#define LCBI_GPU_TOPOLOGY_RETRY 21
 
 #define LCBI_GPU_MODELS_GIVEN 2u  /* points carry model indices into `models` */
 

@@ -481,7 +481,7 @@ int lcbi_gpu_magnification_arrays(lcbi_gpu_context* ctx, int32_t n_sets, const l
 
     const size_t n = static_cast<size_t>(n_times);
     std::vector<double> sx(n), sy(n), a_ps(n);
-    std::vector<int32_t> nimg(n);
+    std::vector<int32_t> nimg(n), levels(n, 0);
     std::vector<lcbi_fs_point> pts(n);
     std::vector<lcbi_fs_result> res(n);
     parallel_sets(n_sets, n_times, [&](int m) {
@@ -490,7 +490,7 @@ int lcbi_gpu_magnification_arrays(lcbi_gpu_context* ctx, int32_t n_sets, const l
     });
     if (n_times > 0) {
         const int rc = lcbi::binary_mag_images(ctx, sts.data(), static_cast<int>(sts.size()), pts.data(), n_times,
-                                               res.data(), a_ps.data(), nimg.data());
+                                               res.data(), a_ps.data(), nimg.data(), levels.data());
         if (rc != LCBI_OK) return rc;
     }
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -514,7 +514,7 @@ int lcbi_gpu_magnification_arrays(lcbi_gpu_context* ctx, int32_t n_sets, const l
             ri.source_y = sy[k0 + i];
             ri.image_count = nimg[k0 + i];
             ri.finite_source_error_estimate = f.error_estimate;
-            ri.finite_source_refinement_level = 0;
+            ri.finite_source_refinement_level = rho == 0.0 ? 0 : levels[k0 + i];
             ri.finite_source_converged = f.converged ? 1 : 0;
             if (!std::isfinite(A)) {
                 status[m] = LCBI_NUMERICAL_ERROR;

@@ -271,6 +271,7 @@ FsWork common_work(Context* ctx)
     w.cell_budget = ctx->cell_budget;
     w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
     w.f32_rays = ctx->f32_rays ? 1 : 0;
+    w.tape = ctx->tape_on ? static_cast<TapeCell*>(ctx->fs_tape.ptr) : nullptr;
     return w;
 }
 
@@ -348,6 +349,8 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     ctx->stage_end(4, ev);
     FsWork r = w;
     r.retry_pass = 1;
+    // The second pass's groups (blocks) have the tapes after the first pass's warps.
+    if (r.tape) r.tape += (long long)ctx->fs_warps * kTapeMax;
     r.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
     r.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
     r.scratch_polar = static_cast<char*>(ctx->fs_scratch_polar_big.ptr);
@@ -383,6 +386,13 @@ bool prepare_tables(Context* ctx, const Plan& plan)
         !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)))
         return false;
     if (ctx->tile_blocks == 0) ctx->tile_blocks = polar_tile_blocks_per_sm() * ctx->sm_count;
+    // Adaptive local refinement needs a tape per scratch group.
+    ctx->tape_on = false;
+    for (const auto& st : plan.settings)
+        if (st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0)) ctx->tape_on = true;
+    if (ctx->tape_on &&
+        !ctx->ensure(ctx->fs_tape, (size_t)(ctx->fs_warps + retry_blocks(ctx)) * kTapeMax * sizeof(TapeCell)))
+        return false;
     if (!ctx->check("ld tables", launch_ld_tables(static_cast<double2*>(ctx->fs_ld_coeffs.ptr), nld,
                                                   static_cast<double*>(ctx->fs_ld.ptr), ctx->stream)))
         return false;
@@ -393,6 +403,9 @@ bool prepare_tables(Context* ctx, const Plan& plan)
 // Per-point ray counts (and cycles) of n points, zeroed.
 bool prepare_counts(Context* ctx, long long n)
 {
+    if (!ctx->ensure(ctx->fs_levels, (size_t)(n + 1) * sizeof(int)) ||
+        !ctx->check("levels init", cudaMemsetAsync(ctx->fs_levels.ptr, 0, (size_t)n * sizeof(int), ctx->stream)))
+        return false;
     if (!ctx->ensure(ctx->fs_rays, (size_t)(n + 1) * sizeof(unsigned long long)) ||
         (ctx->item_cycles && !ctx->ensure(ctx->fs_cycles, (size_t)(n + 1) * sizeof(long long))))
         return false;
@@ -445,6 +458,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = n
         set_lists(w, static_cast<int*>(ctx->fs_counters.ptr), static_cast<int*>(ctx->fs_ir.ptr),
                   static_cast<int*>(ctx->fs_retry.ptr), kChunk, kChunk);
         w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr) + c0;
+        w.levels = static_cast<int*>(ctx->fs_levels.ptr) + c0;
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) + c0 : nullptr;
         if (!stage_decide(ctx, w) || !stage_seeds(ctx, w, cn) || !stage_integrate(ctx, w, cn)) return false;
         if (grads) {
@@ -472,8 +486,10 @@ int finish_results(Context* ctx, lcbi_fs_result* results, long long n)
 bool check_settings(Context* ctx, const lcbi_fs_settings* s, int n)
 {
     for (int i = 0; i < n; ++i) {
-        if (s[i].adaptive_source_bins != 0 && (s[i].finite_source_tol > 0.0 || s[i].finite_source_reltol > 0.0))
-            return ctx->fail("adaptive source bins (local refinement) is not implemented");
+        if (s[i].adaptive_source_bins != 0 && (s[i].finite_source_tol > 0.0 || s[i].finite_source_reltol > 0.0) &&
+            s[i].max_source_bins >= kTapeMax)
+            return ctx->fail("adaptive refinement records at most 4096 boundary cells: max_source_bins must be below "
+                             "4096");
         if (s[i].finite_mode == 3) return ctx->fail("finite_mode 3 (experimental spine integrator) is not implemented");
     }
     return true;
@@ -792,7 +808,7 @@ bool grow_keep(Context* ctx, Buffer& b, size_t bytes)
 // into a store that outlives the pass.
 int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int n_settings,
                       const lcbi_fs_point* points, long long n, lcbi_fs_result* results, double* a_ps,
-                      int32_t* image_count)
+                      int32_t* image_count, int32_t* levels)
 {
     Context* ctx = reinterpret_cast<Context*>(c);
     if (!ctx || n < 0 || !settings || n_settings <= 0) return LCBI_INVALID_ARGUMENT;
@@ -1000,6 +1016,7 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
         set_lists(w, static_cast<int*>(ctx->ir_counters.ptr), static_cast<int*>(ctx->ir_lists.ptr),
                   static_cast<int*>(ctx->ir_retry.ptr), n_cart, n_ir);
         w.rays = static_cast<unsigned long long*>(ctx->fs_rays.ptr);
+        w.levels = static_cast<int*>(ctx->fs_levels.ptr);
         w.cycles = ctx->item_cycles ? static_cast<long long*>(ctx->fs_cycles.ptr) : nullptr;
         if (!stage_seeds(ctx, w, n_ir) || !stage_integrate(ctx, w, n_ir)) return LCBI_GPU_ERROR;
     }
@@ -1009,6 +1026,8 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
                                                 ctx->stream)) ||
         !ctx->check("images D2H", cudaMemcpyAsync(image_count, ctx->fs_all_nimg.ptr, n * sizeof(int32_t),
                                                   cudaMemcpyDeviceToHost, ctx->stream)) ||
+        (levels && !ctx->check("levels D2H", cudaMemcpyAsync(levels, ctx->fs_levels.ptr, n * sizeof(int32_t),
+                                                             cudaMemcpyDeviceToHost, ctx->stream))) ||
         !ctx->finish())
         return LCBI_GPU_ERROR;
     return LCBI_OK;

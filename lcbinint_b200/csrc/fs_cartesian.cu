@@ -129,7 +129,22 @@ struct Ctx {
     int max_steps;
     bool f32;                 // FP32 map about the current seed (A)
     Anchor32 A;
+    // Adaptive local refinement: the point's tape (null: off), kept by rank 0.
+    TapeCell* tape;
+    int tape_n, tape_max;
+    double band, step;
 };
+
+// LocalRefinementTape::add (FSM:993-1003): the first tape_max distinct cells,
+// keyed by their lattice indices, in the order the scan visits them.
+__device__ __noinline__ void tape_add(Ctx& C, double x, double y, double weight)
+{
+    if (C.tape_n >= C.tape_max) return;
+    const long long kx = llround(x / C.step), ky = llround(y / C.step);
+    for (int i = 0; i < C.tape_n; ++i)
+        if (C.tape[i].kx == kx && C.tape[i].ky == ky) return;
+    C.tape[C.tape_n++] = TapeCell{x, y, weight, kx, ky};
+}
 
 // Lens map of one cell, as the reference evaluates it for the current scan.
 __device__ __forceinline__ void eval_for_scan(const Ctx& C, double x, double y, int jsign, double* dz2, double* bright)
@@ -369,6 +384,9 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
         ++cidx;
         rows_ensure<W>(R, yi);
         if (R.ovf) return countall;
+        // Cells near the limb go on the refinement tape (FSM:1952-1961).
+        if (C.tape && Grp<W>::rank() == 0 && fabs(dz2 - C.rho2) <= C.band)
+            tape_add(C, ix, iy, dz2 <= C.rho2 ? b : 0.0);
         if (dz2 <= C.rho2) {
             if (dx == -incr && countx == 0.0) {
                 cur_xmax = ix - dx;
@@ -521,6 +539,189 @@ __device__ __forceinline__ void repair(Ctx& C, RowScratch& R, CartShared<W>& S, 
     if (area0 <= 0.0) --yi;
 }
 
+// ----- adaptive local refinement (fixed_inverse_ray_binary, FSM:3074-3289) -----
+
+struct RefCell {
+    double cx, cy, size, area, coarse, err;
+    int depth;
+    int pad;
+};
+
+// cell_weight (FSM:3088-3095): brightness at a point, 0 outside the source.
+__device__ __forceinline__ double ref_weight(const Ctx& C, double x, double y)
+{
+    const double md2 = mapped_dist2(C.m, x, y, C.src);
+    if (md2 > C.rho2) return 0.0;
+    return C.uniform ? 1.0 : ld_lookup(C.ld, md2 / C.rho2);
+}
+
+// estimate_local_cell_error (FSM:3100-3127).
+__device__ double ref_error(const Ctx& C, const RefCell& c)
+{
+    const double half = 0.5 * c.size;
+    const double xs[4] = {c.cx - half, c.cx + half, c.cx - half, c.cx + half};
+    const double ys[4] = {c.cy - half, c.cy - half, c.cy + half, c.cy + half};
+    double sum = 0.0, lo = dinf(), hi = 0.0;
+    int nonzero = 0;
+    for (int k = 0; k < 4; ++k) {
+        const double wgt = ref_weight(C, xs[k], ys[k]);
+        sum += wgt;
+        lo = (wgt < lo) ? wgt : lo;
+        hi = (hi < wgt) ? wgt : hi;
+        if (wgt > 0.0) ++nonzero;
+    }
+    const double avg = 0.25 * sum;
+    const double center = fabs(avg - c.coarse);
+    const double variation = 0.5 * (hi - lo);
+    const double boundary = (nonzero > 0 && nonzero < 4) ? 0.25 * hi : 0.0;
+    double m = center;
+    if (m < variation) m = variation;
+    if (m < boundary) m = boundary;
+    return c.area * m;
+}
+
+// The binary max-heap of std::priority_queue (ordered by err): push sifts the
+// new cell up past smaller parents; pop moves the last cell into the root's
+// place by walking the hole down to a leaf along the larger child (the right
+// one on ties) and sifting it back up, so cells of equal error leave in the
+// same order as from the reference's queue.
+__device__ void heap_up(RefCell* H, int hole, int top, const RefCell& v)
+{
+    int parent = (hole - 1) / 2;
+    while (hole > top && H[parent].err < v.err) {
+        H[hole] = H[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    H[hole] = v;
+}
+
+__device__ void heap_push(RefCell* H, int& n, const RefCell& v)
+{
+    heap_up(H, n, 0, v);
+    ++n;
+}
+
+__device__ RefCell heap_pop(RefCell* H, int& n)
+{
+    const RefCell top = H[0];
+    if (n > 1) {
+        const RefCell v = H[n - 1];
+        H[n - 1] = H[0];
+        const int len = n - 1;
+        int hole = 0, second = 0;
+        while (second < (len - 1) / 2) {
+            second = 2 * (second + 1);
+            if (H[second].err < H[second - 1].err) --second;
+            H[hole] = H[second];
+            hole = second;
+        }
+        if ((len & 1) == 0 && second == (len - 2) / 2) {
+            second = 2 * (second + 1);
+            H[hole] = H[second - 1];
+            hole = second - 1;
+        }
+        heap_up(H, hole, 0, v);
+    }
+    --n;
+    return top;
+}
+
+struct Refined {
+    double A, err;
+    int level;
+    bool ovf;
+};
+
+// The refinement loop (FSM:3201-3280) over the tape, by one thread; the heap
+// lives in `heap` (capacity `cap` cells).  `err0` is the scan's error estimate.
+__device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, double err0, double scale, int active_bins,
+                          RefCell* heap, int cap)
+{
+    Refined out{A, err0, 0, false};
+    const double safety =
+        st.source_bins < 32 ? 8.0 : (C.rho >= 8.0e-3 ? 2.5 : (C.rho >= 3.0e-3 ? 1.8 : 1.25));
+    auto guarded = [&](double mag) { return (st.tol + st.reltol * dmax_(fabs(mag), 1.0)) / safety; };
+    int n = 0;
+    double lerr = 0.0;
+    for (int i = 0; i < C.tape_n; ++i) {
+        RefCell c{C.tape[i].x, C.tape[i].y, C.step, 1.0, C.tape[i].w, 0.0, 0, 0};
+        c.err = ref_error(C, c);
+        lerr += c.err;
+        if (n >= cap) {
+            out.ovf = true;
+            return out;
+        }
+        heap_push(heap, n, c);
+    }
+    double corr = 0.0;
+    const int max_bins = active_bins > st.max_source_bins ? active_bins : st.max_source_bins;
+    int max_depth = 0;
+    for (int bins = active_bins > 1 ? active_bins : 1; bins < max_bins && max_depth < 8; bins *= 2) ++max_depth;
+    const int max_splits = 4 * max_bins > 64 ? 4 * max_bins : 64;
+    int splits = 0, level = 0;
+    while (n > 0 && lerr > guarded(A + corr / scale) * scale && splits < max_splits) {
+        RefCell parent = heap_pop(heap, n);
+        if (parent.err <= 0.0 || parent.depth >= max_depth) break;
+        int batch = 0;
+        bool defer = false;
+        while (batch < 1 && parent.depth < max_depth && lerr > guarded(A + corr / scale) * scale &&
+               splits < max_splits) {
+            defer = false;
+            // split_cell (FSM:3128-3147).
+            RefCell ch[4];
+            const double size = 0.5 * parent.size;
+            const double off = 0.25 * parent.size;
+            const double cxs[4] = {parent.cx - off, parent.cx + off, parent.cx - off, parent.cx + off};
+            const double cys[4] = {parent.cy - off, parent.cy - off, parent.cy + off, parent.cy + off};
+            double contribution = 0.0, child_err = 0.0;
+            int worst = 0;
+            for (int k = 0; k < 4; ++k) {
+                ch[k] = RefCell{cxs[k], cys[k], size, 0.25 * parent.area, ref_weight(C, cxs[k], cys[k]), 0.0,
+                                parent.depth + 1, 0};
+                ch[k].err = ref_error(C, ch[k]);
+            }
+            for (int k = 0; k < 4; ++k) {
+                contribution += ch[k].area * ch[k].coarse;
+                child_err += ch[k].err;
+                if (ch[k].err > ch[worst].err) worst = k;
+            }
+            const RefCell wc = ch[worst];
+            corr += contribution - parent.area * parent.coarse;
+            lerr += child_err - parent.err;
+            level = level > parent.depth + 1 ? level : parent.depth + 1;
+            ++splits;
+            ++batch;
+            if (n + 4 > cap) {
+                out.ovf = true;
+                return out;
+            }
+            if (lerr <= guarded(A + corr / scale) * scale || wc.err <= 0.0 || wc.depth >= max_depth) {
+                for (int k = 0; k < 4; ++k) heap_push(heap, n, ch[k]);
+                defer = false;
+                break;
+            }
+            for (int k = 0; k < 4; ++k)
+                if (k != worst) heap_push(heap, n, ch[k]);
+            parent = wc;
+            defer = true;
+        }
+        if (defer) {
+            if (n >= cap) {
+                out.ovf = true;
+                return out;
+            }
+            heap_push(heap, n, parent);
+        }
+    }
+    if (level > 0) out.A = A + corr / scale;
+    double e = safety * lerr / scale;
+    if (level == 0 && st.ld_c == 0.0 && st.ld_d == 0.0) e = (e < err0) ? err0 : e;
+    out.err = e;
+    out.level = level;
+    return out;
+}
+
 // The list a kernel instance works through.
 struct CartList {
     const int* slots;   // inverse-ray Cartesian slot of each entry (null: the identity)
@@ -529,7 +730,8 @@ struct CartList {
 };
 
 template <int W>
-__device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S)
+__device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S,
+                               TapeCell* tape)
 {
     constexpr int N = Grp<W>::N;
     const int t = Grp<W>::rank();
@@ -587,6 +789,16 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
             C.f32 = w.f32_rays != 0;
             const double nbin = static_cast<double>(max(st.source_bins, 1));
             const double incr = rho / nbin;
+            // Adaptive local refinement records the scan's boundary cells, so
+            // every cell goes through the reference's loop body (no bulk runs).
+            const bool adaptive = tape && st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0);
+            C.tape = adaptive ? tape : nullptr;
+            C.tape_n = 0;
+            C.tape_max = max(64, st.max_source_bins);
+            if (C.tape_max > kTapeMax) C.tape_max = kTapeMax;
+            C.band = dmax_(4.0 * rho * incr, 4.0 * incr * incr);
+            C.step = incr;
+            if (adaptive) C.bulk = false;
             const double margin = 0.5 * incr * 1.01;
             Diag d{ns, 0, 0, 0, 0, 0, 0.0};
             for (int i = t; i < ns; i += N) {
@@ -736,6 +948,34 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
                 o.err = isfinite(A) ? err : dnan();
                 const double target = st.tol + st.reltol * dmax_(fabs(A), 1.0);
                 o.converged = isfinite(A) && err <= 0.999 * target;
+                if (C.tape && isfinite(A)) {
+                    // needs_global_topology_retry (FSM:1108-1121): the reference
+                    // would scan again at twice the bins; that rerun is not built.
+                    const bool retry = st.source_bins < 50 && st.max_source_bins > st.source_bins && rho < 1.0e-2 &&
+                                       d.seed_count >= 16 && d.overlaps >= 100 && d.gap_repairs >= 1000 &&
+                                       d.max_jump >= 1000.0 &&
+                                       min(st.max_source_bins, max(50, 2 * max(st.source_bins, 1))) > st.source_bins;
+                    Refined rf{A, err, 0, false};
+                    if (!retry && t == 0 && C.tape_n > 0) {
+                        // The row arrays are free once the scans are done: they hold the heap.
+                        rf = refine(C, st, A, err, scale, max(st.source_bins, 1), reinterpret_cast<RefCell*>(R.xmin),
+                                    static_cast<int>((5ll * cap * sizeof(double)) / sizeof(RefCell)));
+                    }
+                    const int active_bins = max(st.source_bins, 1);
+                    if (t == 0) {
+                        if (retry) {
+                            o.status = kFsTopologyRetry;
+                        } else if (rf.ovf) {
+                            o.status = kFsRowOverflow;
+                        } else {
+                            A = rf.A;
+                            o.err = rf.err;
+                            const double tg = st.tol + st.reltol * dmax_(fabs(A), 1.0);
+                            o.converged = rf.err <= 0.999 * tg && active_bins >= 32;
+                            if (w.levels) w.levels[it] = rf.level;
+                        }
+                    }
+                }
             }
         }
         if (ovf && !w.retry_pass) {
@@ -746,7 +986,8 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         }
         o.A = A;
         if (ovf) o.status = kFsRowOverflow;
-        else if (!isfinite(A)) o.status = kFsNumerical;
+        else if (o.status == kFsOk && !isfinite(A)) o.status = kFsNumerical;
+        if (o.status != kFsOk && o.status != kFsNumerical) o.A = dnan();
         if (t == 0) {
             w.out[it] = o;
             if (w.cycles) w.cycles[it] += clock64() - t_item;
@@ -759,14 +1000,16 @@ __global__ void __launch_bounds__(128, 2) cartesian_warp_kernel(FsWork w, unsign
     __shared__ CartShared<1> sh[4];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const CartList L{nullptr, w.ir_count + 0, w.next_item + 1};
-    cartesian_body<1>(w, epoch, L, w.scratch + (long long)gw * w.scratch_per_warp, sh[warp_in_block()]);
+    cartesian_body<1>(w, epoch, L, w.scratch + (long long)gw * w.scratch_per_warp, sh[warp_in_block()],
+                      w.tape ? w.tape + (long long)gw * kTapeMax : nullptr);
 }
 
 __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<kBigWarps> sh;
     const CartList L{w.retry_cart, w.ir_count + 2, w.next_item + 3};
-    cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh);
+    cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
+                              w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr);
 }
 
 } // namespace

@@ -40,6 +40,8 @@ struct Context {
     Buffer pass_raw[2], pass_branches[2], pass_lists[2], pass_counters[2], pass_jobs[2];
     Buffer ir_models, ir_branches, ir_lists, ir_counters, ir_retry;
     Buffer fs_needed, fs_model_base;  // caustic models some point needs; first model of each pass
+    Buffer fs_tape, fs_levels;        // adaptive refinement: boundary-cell tapes; refinement level per point
+    bool tape_on = false;             // the current plan has settings that refine
     void* pinned = nullptr;     // page-locked staging of the passes' work lists and jobs
     size_t pinned_bytes = 0;
     bool trig_ready = false;
@@ -95,7 +97,7 @@ struct Context {
                           &fs_all_aps, &fs_all_nimg, &pass_raw[0], &pass_raw[1], &pass_branches[0],
                           &pass_branches[1], &pass_lists[0], &pass_lists[1], &pass_counters[0], &pass_counters[1],
                           &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry,
-                          &fs_needed, &fs_model_base})
+                          &fs_needed, &fs_model_base, &fs_tape, &fs_levels})
             v.push_back(b);
         return v;
     }

@@ -42,6 +42,16 @@ enum FsStatus {
     kFsRowOverflow = 18,
     kFsQueueOverflow = 19,
     kFsHashOverflow = 20,
+    kFsTopologyRetry = 21,  // adaptive refinement would rerun the scan at twice the bins (not built)
+};
+
+// Adaptive local refinement: the boundary cells a Cartesian scan records
+// (LocalRefinementTape, finite_source_magnifier.cpp:977-1004), at most
+// kTapeMax per point.
+constexpr int kTapeMax = 4096;
+struct TapeCell {
+    double x, y, w;
+    long long kx, ky;
 };
 
 struct FsWork {
@@ -90,6 +100,12 @@ struct FsWork {
     // Inverse-ray cells mapped in FP32 about an image-centred anchor (sums
     // stay FP64); 0: the reference's FP64 map, bit-exact.
     int f32_rays;
+    // Adaptive local refinement (settings with adaptive_source_bins and a
+    // tolerance): one tape of kTapeMax cells per scratch group (indexed as the
+    // scratch areas; null: refinement off), and each point's refinement level
+    // (null: not recorded).
+    TapeCell* tape;
+    int* levels;
 };
 
 constexpr int kBigWarps = 8;

@@ -14,9 +14,10 @@ namespace lcbi {
 // point_source_magnification are ignored; points[i].model is assigned here.
 // Points are processed in chunks that bound the caustic samples held on the
 // device, so per-point separations (lens orbital motion) need no more memory
-// than a chunk's.  results, a_ps and image_count have n entries.
+// than a chunk's.  results, a_ps, image_count and levels (optional: the
+// adaptive refinement level of each point) have n entries.
 int binary_mag_images(lcbi_gpu_context* ctx, const lcbi_fs_settings* settings, int n_settings,
                       const lcbi_fs_point* points, long long n, lcbi_fs_result* results, double* a_ps,
-                      int32_t* image_count);
+                      int32_t* image_count, int32_t* levels);
 
 } // namespace lcbi

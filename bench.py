@@ -813,6 +813,8 @@ def main():
     ap.add_argument("--rays", default="f64", choices=["f64", "f32"],
                     help="fs_batch: lens map of the inverse-ray cells in FP64 (bit-exact) or FP32 about "
                          "image-centred anchors (sums FP64); f32 also reports its error against f64")
+    ap.add_argument("--autotune", action="store_true",
+                    help="fs_batch: launch shapes picked by lcbi_gpu_autotune on the batch before the warm-up")
     ap.add_argument("--no-parallax", action="store_true",
                     help="orbital workload: lens orbital motion only (no annual parallax)")
     ap.add_argument("--models", type=int, default=0,
@@ -917,6 +919,17 @@ def main():
         step_device()
         res64 = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=FS_RESULT_DTYPE)["magnification"].copy()
         L.lcbi_gpu_set_ray_precision(ctx.handle, 32)
+    if args.autotune:
+        # Launch shapes picked on this batch by the library's autotuner.
+        shape = np.zeros(3, dtype=np.int32)
+        best = ctypes_double()
+        rc = L.lcbi_gpu_autotune(ctx.handle, st_arr, len(settings), models.ctypes.data, len(models), n,
+                                 d_pts.data_ptr(), d_res.data_ptr(), _lib.DEVICE_POINTERS | 2, _lib.ptr(shape),
+                                 best.ref())
+        ctx.check(rc, "lcbi_gpu_autotune")
+        config["launch_shape"] = {"tile_flood_blocks_per_sm": int(shape[0]), "warps_per_sm": int(shape[1]),
+                                  "second_pass_blocks": int(shape[2]), "picked_by": "lcbi_gpu_autotune",
+                                  "best_ms": best.value}
     for _ in range(args.warmup):
         flush_l2(flush)
         step_device()

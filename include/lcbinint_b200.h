@@ -211,6 +211,20 @@ int lcbi_gpu_binary_mag(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings,
                         const lcbi_lens_model *models, int32_t n_models, int64_t n,
                         const lcbi_fs_point *points, lcbi_fs_result *results, unsigned flags);
 
+/* Launch-shape autotuner (no reference counterpart).  Runs
+ * lcbi_gpu_binary_mag on the given batch (same arguments and flags) under a
+ * coordinate search of three launch shapes -- blocks per SM of the polar tile
+ * flood fill (1, 2, 4 or the occupancy limit), first-pass warps per SM (4 or
+ * 8) and second-pass blocks (one or two per SM) -- timing each with CUDA events
+ * after one untimed call, and leaves the fastest set on the context.  The
+ * results do not depend on the shapes.  shape (optional) receives {flood
+ * blocks per SM, warps per SM, second-pass blocks}, best_ms the fastest time;
+ * results holds the last call's output. */
+int lcbi_gpu_autotune(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_settings,
+                      const lcbi_lens_model *models, int32_t n_models, int64_t n, const lcbi_fs_point *points,
+                      lcbi_fs_result *results, unsigned flags, int32_t *shape, double *best_ms);
+
+
 /* lcbinint.binary_inverse_ray over n source positions
  * (python/lcbinint_pybind.cpp:3826-3847): the decision thresholds are forced
  * (kinji_threshold 1e18, hex thresholds 0) so every point is integrated by

@@ -146,6 +146,8 @@ def _declare(L):
     L.lcbi_gpu_magnification_arrays.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_uint, _vp,
                                                  _vp]
     L.lcbi_gpu_magnification_arrays.restype = C.c_int
+    L.lcbi_gpu_autotune.argtypes = [_vp, _vp, C.c_int32, _vp, C.c_int32, C.c_int64, _vp, _vp, C.c_uint, _vp, _vp]
+    L.lcbi_gpu_autotune.restype = C.c_int
     L.lcbi_set_earth_ephemeris.argtypes = [C.c_char_p]
     L.lcbi_set_earth_ephemeris.restype = C.c_int
     L.lcbi_gpu_binary_geometry.argtypes = [_vp, C.c_double, C.c_double, C.c_int32, C.c_int32, _vp, _vp]

@@ -599,6 +599,81 @@ int binary_mag_impl(Context* ctx, const lcbi_fs_settings* settings, int32_t n_se
 
 extern "C" {
 
+int lcbi_gpu_autotune(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_settings,
+                      const lcbi_lens_model* models, int32_t n_models, int64_t n, const lcbi_fs_point* points,
+                      lcbi_fs_result* results, unsigned flags, int32_t* shape, double* best_ms)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !settings || n_settings <= 0 || n <= 0 || !points || !results) return LCBI_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaEvent_t e0, e1;
+    if (!ctx->check("event", cudaEventCreate(&e0)) || !ctx->check("event", cudaEventCreate(&e1))) return LCBI_GPU_ERROR;
+    struct Events {
+        cudaEvent_t a, b;
+        ~Events() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } guard{e0, e1};
+    const int sm = ctx->sm_count;
+    const int occupancy = polar_tile_blocks_per_sm();
+    // One shape: {tile flood blocks per SM, first-pass warps per SM, second-pass blocks}.
+    auto apply = [&](const int* sh) {
+        ctx->tile_blocks = sh[0] * sm;
+        ctx->warps_per_sm = sh[1];
+        if (sh[2] != ctx->retry_blocks) {
+            ctx->retry_blocks = sh[2];
+            ctx->big_ready = false;
+        }
+    };
+    // Time of one call with a shape, after one untimed call (allocations, caches).
+    auto measure = [&](const int* sh, double* ms) -> int {
+        apply(sh);
+        int rc = binary_mag_impl(ctx, settings, n_settings, models, n_models, n, points, results, nullptr, flags);
+        if (rc != LCBI_OK) return rc;
+        if (!ctx->check("event", cudaEventRecord(e0, ctx->stream))) return LCBI_GPU_ERROR;
+        rc = binary_mag_impl(ctx, settings, n_settings, models, n_models, n, points, results, nullptr, flags);
+        if (rc != LCBI_OK) return rc;
+        float t = 0.0f;
+        if (!ctx->check("event", cudaEventRecord(e1, ctx->stream)) ||
+            !ctx->check("event", cudaEventSynchronize(e1)) || !ctx->check("event", cudaEventElapsedTime(&t, e0, e1)))
+            return LCBI_GPU_ERROR;
+        *ms = t;
+        return LCBI_OK;
+    };
+    // Coordinate search: flood blocks, then first-pass warps, then second-pass blocks.
+    int best[3] = {occupancy, ctx->warps_per_sm, ctx->retry_blocks > 0 ? ctx->retry_blocks : sm};
+    double best_t = 0.0;
+    int rc = measure(best, &best_t);
+    if (rc != LCBI_OK) return rc;
+    const int floods[4] = {1, 2, 4, occupancy};
+    const int warps[2] = {4, 8};
+    const int seconds[2] = {sm, 2 * sm};
+    for (int axis = 0; axis < 3; ++axis) {
+        const int* cand = axis == 0 ? floods : (axis == 1 ? warps : seconds);
+        const int nc = axis == 0 ? 4 : 2;
+        for (int i = 0; i < nc; ++i) {
+            int sh[3] = {best[0], best[1], best[2]};
+            sh[axis] = cand[i];
+            if (sh[axis] == best[axis] || sh[axis] <= 0) continue;
+            double t = 0.0;
+            rc = measure(sh, &t);
+            if (rc != LCBI_OK) return rc;
+            if (t < best_t) {
+                best_t = t;
+                best[0] = sh[0];
+                best[1] = sh[1];
+                best[2] = sh[2];
+            }
+        }
+    }
+    apply(best);
+    if (shape) {
+        shape[0] = best[0];
+        shape[1] = best[1];
+        shape[2] = best[2];
+    }
+    if (best_ms) *best_ms = best_t;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_binary_inverse_ray(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int64_t n, const double* s,
                                 const double* q, const double* y1, const double* y2, const double* rho, double* A,
                                 int32_t* method, int32_t* status)

@@ -535,6 +535,17 @@ def run_other_workload(args, world, rank, local_rank, ncores):
     launches = ctx.launches - launches0
     if world > 1:
         torch.distributed.barrier()
+    stage_ms = None
+    if args.workload == "light_curve":
+        # Where one curve's time goes: the stages of one more call, CUDA-event timed.
+        L.lcbi_gpu_set_timing(ctx.handle, 1)
+        step_device()
+        sm = np.zeros(8)
+        sn = np.zeros(8, dtype=np.int64)
+        L.lcbi_gpu_stage_times(ctx.handle, _lib.ptr(sm), _lib.ptr(sn), 8)
+        L.lcbi_gpu_set_timing(ctx.handle, 0)
+        names = ["caustics+ld", "decide", "seeds", "cartesian", "polar", "point_source"]
+        stage_ms = {names[i]: float(sm[i]) for i in range(6)}
     e2e_s = 0.0
     for _ in range(args.steps):
         if flush_between:
@@ -551,6 +562,8 @@ def run_other_workload(args, world, rank, local_rank, ncores):
                e2e={"value": n_all * args.steps / max_e2e, "unit": "magnifications/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
                gpu_launches=int(launches), clocks=clocks.summary())
+    if stage_ms is not None:
+        out["stage_ms_one_call"] = stage_ms
     if args.workload == "ps_batch":
         achieved = n * F_PS / (ms_per_step * 1e-3) / 1e12
         out["roofline"] = {"bound": "fp64", "kernel": "ps_batch_kernel", "achieved": achieved, "peak": peak.value,

@@ -59,6 +59,9 @@ Context::~Context()
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
     }
+    if (fork_event) cudaEventDestroy(fork_event);
+    if (join_event) cudaEventDestroy(join_event);
+    if (side_stream) cudaStreamDestroy(side_stream);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -172,8 +175,13 @@ int lcbi_gpu_create(int device, lcbi_gpu_context** out)
     Context* ctx = new (std::nothrow) Context();
     if (!ctx) return LCBI_GPU_ERROR;
     ctx->device = device;
+    int least = 0, greatest = 0;
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->join_event, cudaEventDisableTiming) != cudaSuccess ||
         cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;

@@ -79,6 +79,12 @@ bool ensure_scratch(Context* ctx)
         !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff, pol * warps, ctx->stream)))
         return false;
     ctx->fs_warps = warps;
+    // The scan tags restart with the epoch, so the second-pass scratch, which
+    // still holds tags of the epochs before, is cleared as well (by
+    // ensure_big_scratch, which every caller runs next).  A tag left over
+    // from an earlier scan would otherwise pass for one of the current scan:
+    // rows of another point would join the overlap chains.
+    ctx->big_ready = false;
     ctx->epoch = 0;
     return true;
 }
@@ -338,15 +344,6 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     ctx->stage_begin(3, &ev);
     if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
     ctx->stage_end(3, ev);
-    ctx->stage_begin(4, &ev);
-    if (ctx->polar_tiles) {
-        if (!ctx->check("polar", launch_polar_tiles(w, ctx->fs_tiles.ptr, ctx->tile_capacity, max_points,
-                                                    ctx->tile_blocks, ctx->stream)))
-            return false;
-    } else if (!ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch))) {
-        return false;
-    }
-    ctx->stage_end(4, ev);
     FsWork r = w;
     r.retry_pass = 1;
     // The second pass's groups (blocks) have the tapes after the first pass's warps.
@@ -358,12 +355,46 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     r.row_cap = ctx->row_cap_big;
     r.queue_cap = ctx->queue_cap_big;
     r.hash_cap = ctx->hash_cap_big;
-    ctx->stage_begin(3, &ev);
-    if (!ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
-    ctx->stage_end(3, ev);
+    // The second Cartesian pass often holds one point for hundreds of
+    // milliseconds on one block.  Without stage timing it runs on the side
+    // stream, beside the polar passes, which would otherwise wait for it with
+    // the GPU nearly idle.  The two touch disjoint work lists, counters
+    // (Cartesian: ir_count[0], [2], next_item[1], [3]; polar: ir_count[1],
+    // [3], next_item[2], [4]), outputs and scratch areas, so the results do
+    // not depend on how they interleave.  With stage timing on, the stages run
+    // one after another so that each stage's time is its own.
+    const bool overlap = !ctx->timing && ctx->side_stream != nullptr;
+    if (overlap) {
+        if (!ctx->check("fork", cudaEventRecord(ctx->fork_event, ctx->stream)) ||
+            !ctx->check("fork", cudaStreamWaitEvent(ctx->side_stream, ctx->fork_event, 0)))
+            return false;
+        const bool ok = ctx->check("cartesian retry",
+                                   launch_cartesian(r, retry_blocks(ctx), ctx->side_stream, ctx->epoch));
+        // The join is recorded even after a failed launch, so that the
+        // context's stream never runs ahead of work already queued beside it.
+        if (!ctx->check("join", cudaEventRecord(ctx->join_event, ctx->side_stream)) || !ok) return false;
+    }
     ctx->stage_begin(4, &ev);
-    if (!ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch))) return false;
+    bool polar_ok;
+    if (ctx->polar_tiles) {
+        polar_ok = ctx->check("polar", launch_polar_tiles(w, ctx->fs_tiles.ptr, ctx->tile_capacity, max_points,
+                                                          ctx->tile_blocks, ctx->stream));
+    } else {
+        polar_ok = ctx->check("polar", launch_polar(w, warps, ctx->stream, ctx->epoch));
+    }
     ctx->stage_end(4, ev);
+    if (polar_ok && !overlap) {
+        ctx->stage_begin(3, &ev);
+        polar_ok = ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->stream, ctx->epoch));
+        ctx->stage_end(3, ev);
+    }
+    if (polar_ok) {
+        ctx->stage_begin(4, &ev);
+        polar_ok = ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch));
+        ctx->stage_end(4, ev);
+    }
+    if (overlap && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0))) return false;
+    if (!polar_ok) return false;
     ctx->launches += 8;
     return true;
 }

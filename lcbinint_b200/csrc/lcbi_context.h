@@ -72,6 +72,10 @@ struct Context {
     int grad_bins = 48;
     int grad_blocks = 0;
     cudaStream_t own_stream = nullptr;  // the context's stream; `stream` may be a caller's
+    // Side stream (highest priority) for the second Cartesian pass, which runs
+    // beside the polar passes; fork/join events order it against `stream`.
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t fork_event = nullptr, join_event = nullptr;
 
     // Optional per-stage kernel timing with CUDA events on the launch stream.
     static constexpr int kStages = 8;  // 0 caustics+LD, 1 decide, 2 seeds, 3 cartesian, 4 polar, 5 point source

@@ -68,6 +68,14 @@ int lcbi_gpu_last_item_cycles(lcbi_gpu_context *ctx, int64_t n, int64_t *cycles)
  * a block) for calls of at most 4 points per SM until this is called.  Results
  * are the same for every value. */
 int lcbi_gpu_set_cell_budget(lcbi_gpu_context *ctx, int64_t cells);
+/* Seeding of inverse-ray points (no reference counterpart): a point whose
+ * caustic-crossing phase scan reaches `sources` critical-curve source points
+ * inside its disk (each probed with up to 88 lens-equation solves) is seeded
+ * again by a pass that gives each such point a whole block and probes eight
+ * critical sources at a time.  0 keeps every point on its one warp; the
+ * default is 32.  The seeds, and so the results, are the same for every
+ * value. */
+int lcbi_gpu_set_seed_block_after(lcbi_gpu_context *ctx, int32_t sources);
 /* Precision of the inverse-ray lens map (no reference counterpart; the
  * reference maps every cell in FP64).  64 (the default): the reference's FP64
  * map, bit-exact.  32: each Cartesian scan maps its cells in FP32 about its

@@ -127,6 +127,8 @@ def _declare(L):
     L.lcbi_gpu_set_item_cycles.restype = C.c_int
     L.lcbi_gpu_set_cell_budget.argtypes = [_vp, C.c_int64]
     L.lcbi_gpu_set_cell_budget.restype = C.c_int
+    L.lcbi_gpu_set_seed_block_after.argtypes = [_vp, C.c_int32]
+    L.lcbi_gpu_set_seed_block_after.restype = C.c_int
     L.lcbi_gpu_set_ray_precision.argtypes = [_vp, C.c_int32]
     L.lcbi_gpu_set_ray_precision.restype = C.c_int
     L.lcbi_gpu_set_polar_tiles.argtypes = [_vp, C.c_int]

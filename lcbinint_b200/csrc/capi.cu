@@ -229,6 +229,14 @@ int lcbi_gpu_set_cell_budget(lcbi_gpu_context* c, int64_t cells)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_seed_block_after(lcbi_gpu_context* c, int32_t sources)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || sources < 0) return LCBI_INVALID_ARGUMENT;
+    ctx->seed_block_after = sources;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_set_ray_precision(lcbi_gpu_context* c, int32_t bits)
 {
     Context* ctx = reinterpret_cast<Context*>(c);

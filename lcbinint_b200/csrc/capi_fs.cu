@@ -278,6 +278,9 @@ FsWork common_work(Context* ctx)
     w.few_points = ctx->cell_budget_set ? 0 : 4 * ctx->sm_count;
     w.f32_rays = ctx->f32_rays ? 1 : 0;
     w.tape = ctx->tape_on ? static_cast<TapeCell*>(ctx->fs_tape.ptr) : nullptr;
+    w.seed_block_after = ctx->seed_block_after;
+    w.seed_scratch = static_cast<char*>(ctx->fs_seed_block.ptr);
+    w.seed_scratch_per_block = static_cast<long long>(seed_candidate_bytes_per_warp(ctx->cand_cap));
     return w;
 }
 
@@ -289,6 +292,7 @@ void set_lists(FsWork& w, int* counters, int* lists, int* retry, long long cap_c
     w.ir_polar = lists + cap_cart;
     w.retry_cart = retry;
     w.retry_polar = retry + cap_retry;
+    w.retry_seeds = retry ? retry + 2 * cap_retry : nullptr;
 }
 
 // The decision of every point of w (work lists and counters reset first).
@@ -316,6 +320,12 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
     if (!ctx->check("seeds", launch_seeds(w, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
                                           reinterpret_cast<P2*>(cb + key_bytes * ctx->fs_warps), warps)))
         return false;
+    // The points the one-warp pass handed over (their disks hold many
+    // critical sources), one block each.
+    if (w.seed_block_after > 0 && w.retry_seeds != nullptr && w.seed_scratch != nullptr) {
+        if (!ctx->check("seeds blocks", launch_seeds_blocks(w, retry_blocks(ctx), ctx->stream))) return false;
+        ctx->launches += 1;
+    }
     ctx->stage_end(2, ev);
     return true;
 }
@@ -408,7 +418,9 @@ bool prepare_tables(Context* ctx, const Plan& plan)
         ctx->cand_cap = 4 * plan.max_bins;
         ctx->fs_warps = 0;  // re-size the per-warp areas
     }
-    if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx)) return false;
+    if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx) ||
+        !ctx->ensure(ctx->fs_seed_block, seed_candidate_bytes_per_warp(ctx->cand_cap) * retry_blocks(ctx)))
+        return false;
     const int nld = static_cast<int>(plan.ld_coeffs.size());
     if (!upload(ctx, ctx->fs_settings, plan.settings) || !upload(ctx, ctx->fs_models, plan.models) ||
         !upload(ctx, ctx->fs_raw_offset, plan.raw_offset) || !upload(ctx, ctx->fs_phases, plan.phases) ||
@@ -460,7 +472,7 @@ bool run_pipeline(Context* ctx, const Plan& plan, long long n, double* grads = n
     if (!ctx->ensure(ctx->fs_raw, (raw_total + 1) * sizeof(P2)) ||
         !ctx->ensure(ctx->fs_branches, (raw_total + 1) * sizeof(P2)) ||
         !ctx->ensure(ctx->fs_ir, (size_t)2 * kChunk * sizeof(int)) ||
-        !ctx->ensure(ctx->fs_retry, (size_t)2 * kChunk * sizeof(int)) ||
+        !ctx->ensure(ctx->fs_retry, (size_t)3 * kChunk * sizeof(int)) ||
         !ctx->ensure(ctx->fs_seeds, (size_t)kChunk * ctx->seed_cap * sizeof(P2)) ||
         !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, kChunk)))
         return false;
@@ -1109,7 +1121,7 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
         counters[0] = n_cart;
         counters[1] = n_polar;
         if (!upload(ctx, ctx->ir_lists, lists) || !upload(ctx, ctx->ir_counters, counters) ||
-            !ctx->ensure(ctx->ir_retry, (size_t)2 * n_ir * sizeof(int)) ||
+            !ctx->ensure(ctx->ir_retry, (size_t)3 * n_ir * sizeof(int)) ||
             !ctx->ensure(ctx->fs_seeds, (size_t)n_ir * ctx->seed_cap * sizeof(P2)) ||
             !ctx->ensure(ctx->fs_tiles, tile_bytes(ctx->tile_capacity, n_ir)))
             return LCBI_GPU_ERROR;

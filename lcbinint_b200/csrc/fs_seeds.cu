@@ -77,15 +77,15 @@ __device__ __forceinline__ void probe_batch(SeedState& S, P2 probe, bool active)
     __syncwarp();
 }
 
-// append_valid_probe_image_seeds (FSM:1449-1498) on the solved batch slot `l`.
-__device__ void replay_probe(SeedState& S, int l)
+// append_valid_probe_image_seeds (FSM:1449-1498) on one probe's k candidate
+// images (shared memory, read by the whole warp).
+__device__ void replay_images(SeedState& S, int k, const P2* imgs)
 {
-    const int k = S.sh->cnt[l];
     if (k <= 3) return;
     const int before = S.n;
     const int lim = before < S.cap ? before : S.cap;
     for (int j = 0; j < k; ++j) {
-        const P2 img = S.sh->img[l][j];
+        const P2 img = imgs[j];
         const double md2 = dist2(map_real(S.m, img.x, img.y), S.src);
         if (md2 > S.rho2 * (1.0 + 1.0e-8)) continue;
         int first = -1;
@@ -110,6 +110,9 @@ __device__ void replay_probe(SeedState& S, int l)
         }
     }
 }
+
+// The same on the solved batch slot `l`.
+__device__ __forceinline__ void replay_probe(SeedState& S, int l) { replay_images(S, S.sh->cnt[l], S.sh->img[l]); }
 
 // append_caustic_probe_image_seeds (FSM:1500-1563).
 __device__ void caustic_probe(SeedState& S, P2 cs, const TrigTables& trig)
@@ -310,6 +313,187 @@ __device__ void augment_from_branches(SeedState& S, const CausticModel& md, cons
     }
 }
 
+// Scan position pp of the interleaved caustic-crossing phase scan -> phase sample (FSM:1757-1787).
+__device__ __forceinline__ int phase_sample(int pp)
+{
+    return (pp % (kPhaseSamples / kSkip)) * kSkip + pp / (kPhaseSamples / kSkip);
+}
+
+__device__ __forceinline__ void init_state(SeedState& S, const FsWork& w, int k, const FsItem& item, WarpShared* sh)
+{
+    S.seeds = w.seeds + (long long)k * w.seed_cap;
+    S.cap = w.seed_cap;
+    S.n = 0;
+    S.ovf = false;
+    S.src = P2{item.x, item.y};
+    S.rho = item.rho;
+    S.rho2 = item.rho * item.rho;
+    S.s = item.s;
+    S.q = item.q;
+    S.m = make_mapper(item.s, item.q);
+    S.sh = sh;
+}
+
+// Point images at the source centre (binary_images, point_source_magnifier.cpp:723-737).
+// As seed hints (LensModel, lens_model.cpp:209-226) only the images that
+// map inside the source are kept (append_valid_seed, FSM:1430-1447), all
+// of them if none does (FSM:1722-1727).
+__device__ void initial_seeds(SeedState& S, const FsItem& item)
+{
+    int cnt = 0;
+    if (lane_id() == 0 && item.s != 0.0 && item.q > 0.0) {
+        const BinaryGeom g = make_geom(item.s, item.q, item.x, item.y);
+        dc pos[5];
+        double res[5], det[5];
+        const int all = image_candidates(g, pos, res, det);
+        if (item.flags & kItemSeedHints) {
+            for (int i = 0; i < all; ++i) {
+                if (!(S.rho > 0.0)) break;
+                const P2 mp = map_real(S.m, pos[i].re, pos[i].im);
+                if (dist2(mp, S.src) > S.rho2 * (1.0 + 1.0e-8)) continue;
+                S.seeds[cnt++] = P2{pos[i].re, pos[i].im};
+            }
+        }
+        if (cnt == 0) {
+            for (int i = 0; i < all; ++i) S.seeds[i] = P2{pos[i].re, pos[i].im};
+            cnt = all;
+        }
+    }
+    S.n = shfl_i(cnt, 0);
+    __syncwarp();
+}
+
+// Everything after the caustic-crossing phase scan, on one warp: the refined
+// nearest critical source, the boundary and interior probe rings, the
+// caustic-branch augmentation, and the point's seed count.
+__device__ void finish_seeding(SeedState& S, const FsWork& w, int it, const CausticModel& md, bool found,
+                               double best_d2, double best_phase, long long* ck, P2* cp, long long t_item)
+{
+    if (S.rho > 0.0) {
+        const double phase_step = 2.0 * kPi / static_cast<double>(kPhaseSamples);
+        if (!found && best_d2 < S.rho2 && best_d2 > 0.0) {
+            caustic_probe(S, refine_critical(S, best_phase, phase_step), w.trig);
+        }
+        // Phase 2 (FSM:1800-1865) is not run: its branches start at the
+        // sentinel (1e30, 1e30), whose squared distance to any finite
+        // critical source (about 2e60) never beats the initial bound 1e60,
+        // so no branch is ever assigned and the scan adds no seed.
+        if (S.n < kMaxBoundarySeeds) ring_probes(S, S.rho * (1.0 - 0.02), w.trig.boundary, 400, kMaxBoundarySeeds);
+        if (S.rho >= 2.0e-2) {
+            const double fr[3] = {0.25, 0.5, 0.75};
+            for (int r = 0; r < 3; ++r) ring_probes(S, S.rho * fr[r], w.trig.interior, 64, 0);
+        }
+    }
+    augment_from_branches(S, md, w.branches + md.branch_offset, ck, cp, w.cand_cap);
+    if (lane_id() == 0) {
+        FsOut* o = w.out + it;
+        o->n_seeds = S.n;
+        if (S.ovf) o->status = kFsSeedOverflow;
+        if (w.cycles) w.cycles[it] = clock64() - t_item;
+    }
+    __syncwarp();
+}
+
+// ----- block seeding pass -----
+//
+// A point whose disk holds much of a caustic probes every critical source
+// inside it (8 probes, and 80 more while at most three seeds exist), one
+// source after another; on one warp that is four rounds of lens-quintic
+// solves per source.  The block pass computes the critical sources of all
+// scan positions at once, then the probes of kWinSources consecutive
+// in-disk sources at a time on all its warps, while warp 0 replays the
+// reference's sequential bookkeeping over the solved probes in the
+// reference's order (caustic_probe's early exits included), so the seed list
+// is the same element by element.  Probes solved for sources after the scan
+// stopped are discarded.
+
+constexpr int kScanPositions = kPhaseSamples * 4;
+constexpr int kWinSources = 8;
+constexpr int kProbesPerSource = 88;  // 8 along the caustic normal, 80 on rings (FSM:1500-1563)
+constexpr int kWinProbes = kWinSources * kProbesPerSource;
+constexpr int kCmdWindow = 1, kCmdDone = 2;
+
+struct BlockSeedShared {
+    P2 cs[kPhaseSamples * 4];   // critical source of scan position pp, root i at pp * 4 + i
+    P2 img[kWinProbes][5];      // the window's probe images
+    int cnt[kWinProbes];        // their counts; -1: probe not taken (outside the disk)
+    int win[kWinSources];       // scan positions of the window's sources
+    int n_win;
+    int cmd;
+    int item;
+    WarpShared warp0;
+};
+
+// Named barrier 1 between warp 0 (replay) and the other warps (window
+// solves); the two sides reach it from different places, so it is the
+// unaligned form.
+__device__ __forceinline__ void window_barrier() { asm volatile("barrier.sync 1;" ::: "memory"); }
+
+// Probe j of window source m, as caustic_probe forms and solves it.
+__device__ void window_probe(const SeedState& S, BlockSeedShared& B, int m, int j, const TrigTables& trig)
+{
+    const P2 cs = B.cs[B.win[m]];
+    const double dx = cs.x - S.src.x;
+    const double dy = cs.y - S.src.y;
+    const double dist = hypot_borges(dx, dy);
+    const int slot = m * kProbesPerSource + j;
+    int k = -1;
+    if (dist > 0.0 && dist < S.rho) {
+        P2 p;
+        if (j < 8) {
+            const double steps[4] = {0.02 * S.rho, 0.05 * S.rho, 0.15 * S.rho, 0.35 * S.rho};
+            const double ux = dx / dist;
+            const double uy = dy / dist;
+            const double st = steps[j >> 1];
+            p = (j & 1) ? P2{cs.x - ux * st, cs.y - uy * st} : P2{cs.x + ux * st, cs.y + uy * st};
+        } else {
+            const int idx = j - 8;
+            const double radial[5] = {0.02 * S.rho, 0.05 * S.rho, 0.10 * S.rho, 0.20 * S.rho, 0.35 * S.rho};
+            const double st = radial[idx >> 4];
+            const double2 cssn = trig.angular[idx & 15];
+            p = P2{cs.x + st * cssn.x, cs.y + st * cssn.y};
+        }
+        if (probe_in_disk(S, p)) {
+            k = 0;
+            const BinaryGeom g = make_geom(S.s, S.q, p.x, p.y);
+            dc pos[5];
+            double res[5], det[5];
+            const int nphys = (S.s == 0.0 || S.q <= 0.0) ? -1 : image_candidates(g, pos, res, det);
+            if (nphys > 0) {
+#pragma unroll
+                for (int i = 0; i < 5; ++i) {
+                    if (res[i] * res[i] < 1.0e-12) B.img[slot][k++] = P2{pos[i].re, pos[i].im};
+                }
+            }
+        }
+    }
+    B.cnt[slot] = k;
+}
+
+// caustic_probe (FSM:1500-1563) of window source m on its solved probes (warp 0).
+__device__ void replay_source(SeedState& S, const BlockSeedShared& B, int m)
+{
+    const P2 cs = B.cs[B.win[m]];
+    const double dist = hypot_borges(cs.x - S.src.x, cs.y - S.src.y);
+    if (dist <= 0.0 || dist >= S.rho) return;
+    const int base = m * kProbesPerSource;
+    for (int l = 0; l < 8; ++l)
+        if (B.cnt[base + l] >= 0) replay_images(S, B.cnt[base + l], B.img[base + l]);
+    if (S.n <= 3) {
+        for (int idx = 0; idx < 80; ++idx) {
+            const int sl = base + 8 + idx;
+            if (B.cnt[sl] >= 0) replay_images(S, B.cnt[sl], B.img[sl]);
+            if (S.n > 3) return;
+        }
+    }
+}
+
+__device__ __forceinline__ bool in_disk_source(const SeedState& S, P2 cs)
+{
+    const double d2 = dist2(cs, S.src);
+    return !(d2 >= S.rho2 || d2 <= 0.0);
+}
+
 } // namespace
 
 __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_keys, P2* cand_probes)
@@ -321,6 +505,7 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
     P2* cp = cand_probes + (long long)gw * 2 * w.cand_cap;
     const int n_cart = w.ir_count[0];
     const int total = n_cart + w.ir_count[1];
+    const bool can_hand_over = w.seed_block_after > 0 && w.retry_seeds != nullptr;
     for (;;) {
         int k = 0;
         if (lane_id() == 0) k = atomicAdd(&w.next_item[0], 1);
@@ -331,66 +516,29 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
         const FsItem item = w.items[it];
         const CausticModel md = w.models[item.model];
         SeedState S;
-        S.seeds = w.seeds + (long long)k * w.seed_cap;
-        S.cap = w.seed_cap;
-        S.n = 0;
-        S.ovf = false;
-        S.src = P2{item.x, item.y};
-        S.rho = item.rho;
-        S.rho2 = item.rho * item.rho;
-        S.s = item.s;
-        S.q = item.q;
-        S.m = make_mapper(item.s, item.q);
-        S.sh = sh;
-
-        // Point images at the source centre (binary_images, point_source_magnifier.cpp:723-737).
-        // As seed hints (LensModel, lens_model.cpp:209-226) only the images that
-        // map inside the source are kept (append_valid_seed, FSM:1430-1447), all
-        // of them if none does (FSM:1722-1727).
-        {
-            int cnt = 0;
-            if (lane_id() == 0 && item.s != 0.0 && item.q > 0.0) {
-                const BinaryGeom g = make_geom(item.s, item.q, item.x, item.y);
-                dc pos[5];
-                double res[5], det[5];
-                const int all = image_candidates(g, pos, res, det);
-                if (item.flags & kItemSeedHints) {
-                    for (int i = 0; i < all; ++i) {
-                        if (!(S.rho > 0.0)) break;
-                        const P2 mp = map_real(S.m, pos[i].re, pos[i].im);
-                        if (dist2(mp, S.src) > S.rho2 * (1.0 + 1.0e-8)) continue;
-                        S.seeds[cnt++] = P2{pos[i].re, pos[i].im};
-                    }
-                }
-                if (cnt == 0) {
-                    for (int i = 0; i < all; ++i) S.seeds[i] = P2{pos[i].re, pos[i].im};
-                    cnt = all;
-                }
-            }
-            S.n = shfl_i(cnt, 0);
-            __syncwarp();
-        }
+        init_state(S, w, k, item, sh);
+        initial_seeds(S, item);
+        double best_d2 = dinf();
+        double best_phase = 0.0;
+        bool found = false;
+        bool hand_over = false;
         if (S.rho > 0.0) {
             // Phase 1: interleaved phase scan for the first caustic crossing (FSM:1757-1787).
             const double phase_step = 2.0 * kPi / static_cast<double>(kPhaseSamples);
-            double best_d2 = dinf();
-            double best_phase = 0.0;
-            bool found = false;
-            for (int p0 = 0; p0 < kPhaseSamples && !found; p0 += 32) {
+            int reached = 0;  // critical sources inside the disk met so far
+            for (int p0 = 0; p0 < kPhaseSamples && !found && !hand_over; p0 += 32) {
                 const int pl = p0 + lane_id();
                 P2 c[4];
                 if (pl < kPhaseSamples) {
-                    const int sample = (pl % (kPhaseSamples / kSkip)) * kSkip + pl / (kPhaseSamples / kSkip);
-                    const double2 ph = w.trig.seed_phase[sample];
+                    const double2 ph = w.trig.seed_phase[phase_sample(pl)];
                     dc roots[4];
                     critical_roots(S.s, S.q, dc{ph.x, ph.y}, roots);
 #pragma unroll
                     for (int i = 0; i < 4; ++i) c[i] = map_real(S.m, roots[i].re, roots[i].im);
                 }
-                for (int l = 0; l < 32 && p0 + l < kPhaseSamples && !found; ++l) {
+                for (int l = 0; l < 32 && p0 + l < kPhaseSamples && !found && !hand_over; ++l) {
                     const int pp = p0 + l;
-                    const int sample = (pp % (kPhaseSamples / kSkip)) * kSkip + pp / (kPhaseSamples / kSkip);
-                    const double phi = phase_step * static_cast<double>(sample);
+                    const double phi = phase_step * static_cast<double>(phase_sample(pp));
                     for (int i = 0; i < 4; ++i) {
                         const P2 cs{shfl_d(c[i].x, l), shfl_d(c[i].y, l)};
                         const double d2 = dist2(cs, S.src);
@@ -399,33 +547,125 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
                             best_phase = phi;
                         }
                         if (d2 >= S.rho2 || d2 <= 0.0) continue;
+                        if (can_hand_over && ++reached >= w.seed_block_after) {
+                            hand_over = true;
+                            break;
+                        }
                         const int before = S.n;
                         caustic_probe(S, cs, w.trig);
                         found = S.n > before;
                     }
                 }
             }
-            if (!found && best_d2 < S.rho2 && best_d2 > 0.0) {
-                caustic_probe(S, refine_critical(S, best_phase, phase_step), w.trig);
+        }
+        if (hand_over) {
+            // The block pass seeds the point again from the start.
+            if (lane_id() == 0) w.retry_seeds[atomicAdd(&w.ir_count[4], 1)] = k;
+            __syncwarp();
+            continue;
+        }
+        finish_seeding(S, w, it, md, found, best_d2, best_phase, ck, cp, t_item);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kBigWarps, 1) seeds_block_kernel(FsWork w)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    BlockSeedShared& B = *reinterpret_cast<BlockSeedShared*>(smem);
+    const int t = threadIdx.x;
+    const int nt = blockDim.x;
+    long long* ck = reinterpret_cast<long long*>(w.seed_scratch + (long long)blockIdx.x * w.seed_scratch_per_block);
+    P2* cp = reinterpret_cast<P2*>(ck + 2 * (long long)w.cand_cap);
+    const int n = w.ir_count[4];
+    const int n_cart = w.ir_count[0];
+    for (;;) {
+        __syncthreads();
+        if (t == 0) B.item = atomicAdd(&w.next_item[5], 1);
+        __syncthreads();
+        const int r = B.item;
+        if (r >= n) break;
+        const int k = w.retry_seeds[r];
+        const int it = (k < n_cart) ? w.ir_cart[k] : w.ir_polar[k - n_cart];
+        const long long t_item = clock64();
+        const FsItem item = w.items[it];
+        SeedState S;
+        init_state(S, w, k, item, &B.warp0);
+        // Critical sources of every scan position, all threads.
+        for (int pp = t; pp < kPhaseSamples; pp += nt) {
+            const double2 ph = w.trig.seed_phase[phase_sample(pp)];
+            dc roots[4];
+            critical_roots(S.s, S.q, dc{ph.x, ph.y}, roots);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) B.cs[pp * 4 + i] = map_real(S.m, roots[i].re, roots[i].im);
+        }
+        __syncthreads();
+        if (warp_in_block() != 0) {
+            // Window solves on request of warp 0.
+            for (;;) {
+                window_barrier();
+                if (B.cmd == kCmdDone) break;
+                for (int g = t; g < B.n_win * kProbesPerSource; g += nt)
+                    window_probe(S, B, g / kProbesPerSource, g % kProbesPerSource, w.trig);
+                window_barrier();
             }
-            // Phase 2 (FSM:1800-1865) is not run: its branches start at the
-            // sentinel (1e30, 1e30), whose squared distance to any finite
-            // critical source (about 2e60) never beats the initial bound 1e60,
-            // so no branch is ever assigned and the scan adds no seed.
-            if (S.n < kMaxBoundarySeeds) ring_probes(S, S.rho * (1.0 - 0.02), w.trig.boundary, 400, kMaxBoundarySeeds);
-            if (S.rho >= 2.0e-2) {
-                const double fr[3] = {0.25, 0.5, 0.75};
-                for (int r = 0; r < 3; ++r) ring_probes(S, S.rho * fr[r], w.trig.interior, 64, 0);
+            continue;
+        }
+        const CausticModel md = w.models[item.model];
+        initial_seeds(S, item);
+        double best_d2 = dinf();
+        double best_phase = 0.0;
+        bool found = false;
+        if (S.rho > 0.0) {
+            const double phase_step = 2.0 * kPi / static_cast<double>(kPhaseSamples);
+            int win_end = 0;  // scan positions before win_end that lie in the disk are in the window
+            int m = 0;        // window source the replay is at
+            for (int pp = 0; pp < kPhaseSamples && !found; ++pp) {
+                const double phi = phase_step * static_cast<double>(phase_sample(pp));
+                for (int i = 0; i < 4; ++i) {
+                    const int pos = pp * 4 + i;
+                    const P2 cs = B.cs[pos];
+                    const double d2 = dist2(cs, S.src);
+                    if (d2 < best_d2) {
+                        best_d2 = d2;
+                        best_phase = phi;
+                    }
+                    if (d2 >= S.rho2 || d2 <= 0.0) continue;
+                    if (pos >= win_end) {
+                        // The next kWinSources in-disk sources from pos on, in scan order.
+                        int nw = 0, last_pos = pos;
+                        for (int q = pos; q < kScanPositions && nw < kWinSources; q += 32) {
+                            const int qq = q + lane_id();
+                            const bool in = qq < kScanPositions && in_disk_source(S, B.cs[qq]);
+                            unsigned bal = __ballot_sync(kFull, in);
+                            while (__popc(bal) > kWinSources - nw) bal &= ~(1u << (31 - __clz(bal)));
+                            if ((bal >> lane_id()) & 1u) B.win[nw + __popc(bal & ((1u << lane_id()) - 1u))] = qq;
+                            if (bal) last_pos = q + 31 - __clz(bal);
+                            nw += __popc(bal);
+                        }
+                        // In-disk positions before win_end are all in the window.
+                        win_end = nw == kWinSources ? last_pos + 1 : kScanPositions;
+                        if (lane_id() == 0) {
+                            B.n_win = nw;
+                            B.cmd = kCmdWindow;
+                        }
+                        __syncwarp();
+                        window_barrier();
+                        for (int g = t; g < nw * kProbesPerSource; g += nt)
+                            window_probe(S, B, g / kProbesPerSource, g % kProbesPerSource, w.trig);
+                        window_barrier();
+                        m = 0;
+                    }
+                    while (m + 1 < B.n_win && B.win[m] != pos) ++m;
+                    const int before = S.n;
+                    replay_source(S, B, m);
+                    found = S.n > before;
+                }
             }
         }
-        augment_from_branches(S, md, w.branches + md.branch_offset, ck, cp, w.cand_cap);
-        if (lane_id() == 0) {
-            FsOut* o = w.out + it;
-            o->n_seeds = S.n;
-            if (S.ovf) o->status = kFsSeedOverflow;
-            if (w.cycles) w.cycles[it] = clock64() - t_item;
-        }
+        if (lane_id() == 0) B.cmd = kCmdDone;
         __syncwarp();
+        window_barrier();
+        finish_seeding(S, w, it, md, found, best_d2, best_phase, ck, cp, t_item);
     }
 }
 
@@ -436,6 +676,15 @@ cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, lon
     const size_t smem = 4 * sizeof(WarpShared);
     seeds_kernel<<<blocks, 128, smem, stream>>>(w, cand_keys, cand_probes);
     (void)sm_count;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seeds_blocks(const FsWork& w, int n_blocks, cudaStream_t stream)
+{
+    const int smem = static_cast<int>(sizeof(BlockSeedShared));
+    cudaError_t e = cudaFuncSetAttribute(seeds_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    seeds_block_kernel<<<n_blocks, 32 * kBigWarps, smem, stream>>>(w);
     return cudaGetLastError();
 }
 

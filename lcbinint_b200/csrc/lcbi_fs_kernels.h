@@ -106,6 +106,16 @@ struct FsWork {
     // (null: not recorded).
     TapeCell* tape;
     int* levels;
+    // Seeding: a point whose caustic-crossing phase scan reaches this many
+    // critical sources inside its disk (0: no limit) is handed from the
+    // one-warp seeding pass to the block seeding pass (launch_seeds_blocks),
+    // which probes several critical sources at once.  Its list position goes
+    // to retry_seeds (count in ir_count[4]); each block of that pass has
+    // seed_scratch_per_block bytes of candidate scratch at seed_scratch.
+    int seed_block_after;
+    int* retry_seeds;
+    char* seed_scratch;
+    long long seed_scratch_per_block;
 };
 
 constexpr int kBigWarps = 8;
@@ -134,6 +144,8 @@ cudaError_t launch_polar_tiles(const FsWork& w, void* area, long long capacity, 
 size_t tile_bytes(long long capacity, int max_items);
 int polar_tile_blocks_per_sm();
 size_t seed_candidate_bytes_per_warp(int cand_cap);
+// Block seeding pass over w.retry_seeds: n_blocks blocks of kBigWarps warps.
+cudaError_t launch_seeds_blocks(const FsWork& w, int n_blocks, cudaStream_t stream);
 // Adjoint: dA/d(y1, y2, s, q, rho, c), the value differentiated and the method
 // of every point of the work lists (8 doubles per point).
 cudaError_t launch_grad(const FsWork& w, void* area, long long capacity, int max_items, int flood_blocks,

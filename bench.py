@@ -826,6 +826,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N points (small cases for profiler captures)")
+    ap.add_argument("--point", type=int, default=-1,
+                    help="fs_batch: only point N of the batch, on a second-pass block (cell budget 1), with a "
+                         "small workspace (one first-pass warp per SM, two second-pass blocks): the one-kernel "
+                         "case for profiler captures of the block scan (point 1285: the batch's largest "
+                         "Cartesian point)")
     ap.add_argument("--rays", default="f64", choices=["f64", "f32"],
                     help="fs_batch: lens map of the inverse-ray cells in FP64 (bit-exact) or FP32 about "
                          "image-centred anchors (sums FP64); f32 also reports its error against f64")
@@ -848,6 +853,8 @@ def main():
     rows = fs_batch_workload(seed=1 + rank)
     if args.points > 0:
         rows = rows[np.random.default_rng(5).permutation(len(rows))[: args.points]]
+    if args.point >= 0:
+        rows = rows[[args.point]]
     config = {"workload": "fs_batch: 4096 forced inverse-ray points, 64 models x 64 epochs, "
                           "Cartesian/polar mixed, nbin 20-200, linear LD",
               "points": int(len(rows)), "models": 64,
@@ -893,6 +900,9 @@ def main():
     L = ctx._L
     stream = torch.cuda.current_stream(dev)
     L.lcbi_gpu_set_stream(ctx.handle, stream.cuda_stream)
+    if args.point >= 0:
+        ctx.check(L.lcbi_gpu_set_cell_budget(ctx.handle, 1), "lcbi_gpu_set_cell_budget")
+        ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 2, 16384), "lcbi_gpu_set_workspace")
 
     settings, sidx = fs_settings_for(rows)
     st_arr = (LcbiStructs.FsSettings * len(settings))(*settings)

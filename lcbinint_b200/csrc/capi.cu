@@ -62,6 +62,9 @@ Context::~Context()
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     if (side_stream) cudaStreamDestroy(side_stream);
+    if (early_fork) cudaEventDestroy(early_fork);
+    if (early_join) cudaEventDestroy(early_join);
+    if (early_stream) cudaStreamDestroy(early_stream);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -182,6 +185,9 @@ int lcbi_gpu_create(int device, lcbi_gpu_context** out)
         cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->join_event, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->early_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->early_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->early_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;

@@ -97,7 +97,8 @@ int retry_blocks(const Context* c) { return c->retry_blocks > 0 ? c->retry_block
 bool ensure_big_scratch(Context* ctx)
 {
     if (ctx->big_ready) return true;
-    const size_t cb = cart_bytes_big(ctx) * retry_blocks(ctx);
+    // Cartesian: the second pass's blocks, then kEarlyMax blocks of the early pass.
+    const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + kEarlyMax);
     const size_t pb = polar_bytes_big(ctx) * retry_blocks(ctx);
     if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb)) return false;
     if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_big.ptr, 0xff, cb, ctx->stream)) ||
@@ -293,6 +294,7 @@ void set_lists(FsWork& w, int* counters, int* lists, int* retry, long long cap_c
     w.retry_cart = retry;
     w.retry_polar = retry + cap_retry;
     w.retry_seeds = retry ? retry + 2 * cap_retry : nullptr;
+    w.early_cart = counters + 16;  // counters[16, 16 + kEarlyMax); the candidate count is counters[48]
 }
 
 // The decision of every point of w (work lists and counters reset first).
@@ -350,7 +352,40 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         ctx->epoch = 1;
     }
     const int warps = ctx->fs_warps < max_points ? ctx->fs_warps : max_points;
+    const bool overlap = !ctx->timing && ctx->side_stream != nullptr && ctx->early_stream != nullptr;
     cudaEvent_t ev;
+    // Cartesian points predicted to pass the first pass's cell budget four
+    // times over or more would spend the whole budget on their warp before
+    // starting again on a block.  They run on blocks from the start instead,
+    // on the early stream beside the first pass, which skips them (largest
+    // first; their own scratch blocks after the second pass's).  Adaptive
+    // refinement keeps one tape per group and does not use this path.
+    const bool early = ctx->cell_budget > 0 && w.tape == nullptr && w.early_cart != nullptr;
+    if (early) {
+        if (!ctx->check("route", launch_route_early(w, 4.0 * static_cast<double>(ctx->cell_budget),
+                                                    ctx->fs_route.ptr, max_points, ctx->sm_count, ctx->stream)))
+            return false;
+        FsWork e = w;
+        e.retry_pass = 1;
+        e.early_pass = 1;
+        e.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr) +
+                    (long long)retry_blocks(ctx) * static_cast<long long>(cart_bytes_big(ctx));
+        e.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
+        e.row_cap = ctx->row_cap_big;
+        if (overlap) {
+            if (!ctx->check("fork", cudaEventRecord(ctx->early_fork, ctx->stream)) ||
+                !ctx->check("fork", cudaStreamWaitEvent(ctx->early_stream, ctx->early_fork, 0)))
+                return false;
+            const bool ok = ctx->check("cartesian early",
+                                       launch_cartesian(e, kEarlyMax, ctx->early_stream, ctx->epoch));
+            if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream)) || !ok) return false;
+        } else {
+            ctx->stage_begin(3, &ev);
+            if (!ctx->check("cartesian early", launch_cartesian(e, kEarlyMax, ctx->stream, ctx->epoch))) return false;
+            ctx->stage_end(3, ev);
+        }
+        ctx->launches += 3;
+    }
     ctx->stage_begin(3, &ev);
     if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
     ctx->stage_end(3, ev);
@@ -373,7 +408,6 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     // [3], next_item[2], [4]), outputs and scratch areas, so the results do
     // not depend on how they interleave.  With stage timing on, the stages run
     // one after another so that each stage's time is its own.
-    const bool overlap = !ctx->timing && ctx->side_stream != nullptr;
     if (overlap) {
         if (!ctx->check("fork", cudaEventRecord(ctx->fork_event, ctx->stream)) ||
             !ctx->check("fork", cudaStreamWaitEvent(ctx->side_stream, ctx->fork_event, 0)))
@@ -404,6 +438,7 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         ctx->stage_end(4, ev);
     }
     if (overlap && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0))) return false;
+    if (overlap && early && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
     if (!polar_ok) return false;
     ctx->launches += 8;
     return true;
@@ -419,7 +454,8 @@ bool prepare_tables(Context* ctx, const Plan& plan)
         ctx->fs_warps = 0;  // re-size the per-warp areas
     }
     if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx) ||
-        !ctx->ensure(ctx->fs_seed_block, seed_candidate_bytes_per_warp(ctx->cand_cap) * retry_blocks(ctx)))
+        !ctx->ensure(ctx->fs_seed_block, seed_candidate_bytes_per_warp(ctx->cand_cap) * retry_blocks(ctx)) ||
+        !ctx->ensure(ctx->fs_route, route_bytes()))
         return false;
     const int nld = static_cast<int>(plan.ld_coeffs.size());
     if (!upload(ctx, ctx->fs_settings, plan.settings) || !upload(ctx, ctx->fs_models, plan.models) ||

@@ -760,6 +760,13 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         int k = S.item;
         if (k >= n) break;
         if (L.slots) k = L.slots[k];
+        if (W == 1 && !w.retry_pass && w.early_cart != nullptr) {
+            // Points routed to the early block pass are not run here.
+            const int ne = w.ir_count[5];
+            bool routed = false;
+            for (int e = 0; e < ne; ++e) routed |= w.early_cart[e] == k;
+            if (routed) continue;
+        }
         const int it = w.ir_cart[k];
         const long long t_item = clock64();
         const FsItem item = w.items[it];
@@ -1007,7 +1014,8 @@ __global__ void __launch_bounds__(128, 2) cartesian_warp_kernel(FsWork w, unsign
 __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<kBigWarps> sh;
-    const CartList L{w.retry_cart, w.ir_count + 2, w.next_item + 3};
+    const CartList L = w.early_pass ? CartList{w.early_cart, w.ir_count + 5, w.next_item + 6}
+                                    : CartList{w.retry_cart, w.ir_count + 2, w.next_item + 3};
     cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
                               w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr);
 }

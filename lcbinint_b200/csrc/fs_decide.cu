@@ -216,4 +216,68 @@ cudaError_t launch_decide(const FsWork& w, int sm_count, cudaStream_t stream)
     return cudaGetLastError();
 }
 
+// ----- early block routing of large Cartesian points -----
+//
+// A Cartesian point's in-source cell count is about pi nbin^2 |A| (image area
+// A pi rho^2 over cells of (rho / nbin)^2); with the point-source A in place
+// of the finite-source one this ranked the largest point of the 4,096-point
+// fs_batch first, at its exact count.  The prediction only decides where a
+// point runs (the block pass gives the first pass's results bit for bit),
+// never what it returns.
+
+struct RouteCand {
+    int k;
+    int pad;
+    double est;
+};
+
+__global__ void __launch_bounds__(128) route_estimate_kernel(FsWork w, double min_cells, RouteCand* cand, int* ncand)
+{
+    const int n = w.ir_count[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int it = w.ir_cart[k];
+        const FsOut o = w.out[it];
+        const FsItem item = w.items[it];
+        if (o.status != kFsOk || o.n_seeds <= 0 || !(item.rho > 0.0)) continue;
+        const FsSettingsDev st = w.settings[item.settings];
+        const double nbin = static_cast<double>(max(st.source_bins, 1));
+        const double a = point_source(item.s, item.q, item.x, item.y).magnification;
+        const double est = kPi * nbin * nbin * dmax_(fabs(a), 1.0);
+        if (est > min_cells) {
+            const int c = atomicAdd(ncand, 1);
+            if (c < kRouteCands) cand[c] = RouteCand{k, 0, est};
+        }
+    }
+}
+
+// The kEarlyMax largest candidates, largest first (ties by list position).
+__global__ void __launch_bounds__(256) route_select_kernel(FsWork w, const RouteCand* cand, const int* ncand)
+{
+    const int m = min(*ncand, kRouteCands);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const RouteCand c = cand[i];
+        int rank = 0;
+        for (int j = 0; j < m; ++j) {
+            const RouteCand o = cand[j];
+            rank += (o.est > c.est || (o.est == c.est && o.k < c.k)) ? 1 : 0;
+        }
+        if (rank < kEarlyMax) w.early_cart[rank] = c.k;
+    }
+    if (threadIdx.x == 0) w.ir_count[5] = min(m, kEarlyMax);
+}
+
+size_t route_bytes() { return (size_t)kRouteCands * sizeof(RouteCand); }
+
+cudaError_t launch_route_early(const FsWork& w, double min_cells, void* cand, int max_points, int sm_count,
+                               cudaStream_t stream)
+{
+    if (max_points <= 0) return cudaSuccess;
+    int blocks = (max_points + 127) / 128;
+    if (blocks > 4 * sm_count) blocks = 4 * sm_count;
+    int* ncand = w.ir_count + 48;
+    route_estimate_kernel<<<blocks, 128, 0, stream>>>(w, min_cells, static_cast<RouteCand*>(cand), ncand);
+    route_select_kernel<<<1, 256, 0, stream>>>(w, static_cast<const RouteCand*>(cand), ncand);
+    return cudaGetLastError();
+}
+
 } // namespace lcbi

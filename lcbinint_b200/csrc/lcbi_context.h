@@ -42,6 +42,7 @@ struct Context {
     Buffer fs_needed, fs_model_base;  // caustic models some point needs; first model of each pass
     Buffer fs_tape, fs_levels;        // adaptive refinement: boundary-cell tapes; refinement level per point
     Buffer fs_seed_block;             // block seeding pass: candidate scratch per block
+    Buffer fs_route;                  // early block routing: candidate list
     int seed_block_after = 32;        // in-disk critical sources that move a point's seeding to a block (0: never)
     bool tape_on = false;             // the current plan has settings that refine
     void* pinned = nullptr;     // page-locked staging of the passes' work lists and jobs
@@ -78,6 +79,10 @@ struct Context {
     // beside the polar passes; fork/join events order it against `stream`.
     cudaStream_t side_stream = nullptr;
     cudaEvent_t fork_event = nullptr, join_event = nullptr;
+    // Early stream (highest priority) for the Cartesian points routed to
+    // blocks from the start, beside the first pass.
+    cudaStream_t early_stream = nullptr;
+    cudaEvent_t early_fork = nullptr, early_join = nullptr;
 
     // Optional per-stage kernel timing with CUDA events on the launch stream.
     static constexpr int kStages = 8;  // 0 caustics+LD, 1 decide, 2 seeds, 3 cartesian, 4 polar, 5 point source
@@ -102,7 +107,7 @@ struct Context {
                           &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc,
                           &fs_all_aps, &fs_all_nimg, &pass_raw[0], &pass_raw[1], &pass_branches[0],
                           &pass_branches[1], &pass_lists[0], &pass_lists[1], &pass_counters[0], &pass_counters[1],
-                          &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry, &fs_seed_block,
+                          &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry, &fs_seed_block, &fs_route,
                           &fs_needed, &fs_model_base, &fs_tape, &fs_levels})
             v.push_back(b);
         return v;

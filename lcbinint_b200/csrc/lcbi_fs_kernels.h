@@ -116,7 +116,16 @@ struct FsWork {
     int* retry_seeds;
     char* seed_scratch;
     long long seed_scratch_per_block;
+    // Cartesian points predicted to pass the first pass's budget many times
+    // over (launch_route_early) run on blocks from the start, beside the first
+    // pass, which skips them: their list positions, largest first, at
+    // early_cart (count in ir_count[5], at most kEarlyMax).  early_pass = 1
+    // makes the block kernel take that list (work counter next_item[6]).
+    int* early_cart;
+    int early_pass;
 };
+
+constexpr int kEarlyMax = 32;
 
 constexpr int kBigWarps = 8;
 
@@ -136,6 +145,14 @@ cudaError_t launch_decide(const FsWork& w, int sm_count, cudaStream_t stream);
 cudaError_t launch_seeds(const FsWork& w, int sm_count, cudaStream_t stream, long long* cand_keys, P2* cand_probes,
                          int n_warps);
 cudaError_t launch_cartesian(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
+// Picks the early Cartesian points (predicted in-source cells
+// pi nbin^2 max(|A_ps|, 1) above min_cells), at most kEarlyMax, largest first,
+// into w.early_cart and ir_count[5]; `cand` holds route_bytes() of candidates,
+// counted in ir_count[48] (zero beforehand).
+constexpr int kRouteCands = 1024;
+size_t route_bytes();
+cudaError_t launch_route_early(const FsWork& w, double min_cells, void* cand, int max_points, int sm_count,
+                               cudaStream_t stream);
 cudaError_t launch_polar(const FsWork& w, int n_warps, cudaStream_t stream, unsigned long long epoch);
 // Tile-parallel polar flood fill of every polar point of the work lists
 // (first pass); points that do not fit go to the second-pass retry list.

@@ -93,3 +93,36 @@ def test_workspace_resize_keeps_second_pass_results():
     for _ in range(2):
         got = run(ctx, rng.permutation(len(rows)))
         assert got.tobytes() == fresh.tobytes()
+
+
+def test_early_block_routing_keeps_results():
+    """Cartesian points predicted to need many times the first pass's cell
+    budget run on blocks from the start, beside the first pass.  Routing
+    changes where a point runs, not what it returns: no routing (budget 0,
+    every point on its warp), heavy routing (a small budget, so the 32 largest
+    predicted points go early) and the default give the same bytes."""
+    import bench
+    from lcbinint_b200 import _lib
+    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, LcbiStructs, PS_EXACT, PS_ON_DEVICE
+    rows = bench.fs_batch_workload(seed=7)
+    rows = rows[rows[:, 7] <= 100]  # keep every point small enough for one warp without a budget
+    rows = rows[np.random.default_rng(14).permutation(len(rows))[:320]]
+    settings, sidx = bench.fs_settings_for(rows)
+    st = (LcbiStructs.FsSettings * len(settings))(*settings)
+    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
+    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
+    pts["settings"] = sidx
+    pts["flags"] = PS_EXACT | PS_ON_DEVICE
+    outs = {}
+    for budget in (0, 1 << 12, 1 << 19):
+        ctx = _lib.Context(0)
+        assert ctx._L.lcbi_gpu_set_cell_budget(ctx.handle, budget) == 0
+        out = np.zeros(len(rows), dtype=FS_RESULT_DTYPE)
+        ctx.check(ctx._L.lcbi_gpu_binary_mag(ctx.handle, st, len(settings), None, 0, len(rows), pts.ctypes.data,
+                                             out.ctypes.data, 0), "lcbi_gpu_binary_mag")
+        outs[budget] = out
+    base = outs[0]
+    assert (base["status"] == 0).all()
+    assert (base["method"] == 2).any()
+    for budget in (1 << 12, 1 << 19):
+        assert outs[budget].tobytes() == base.tobytes(), budget

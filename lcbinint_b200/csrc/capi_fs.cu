@@ -308,24 +308,109 @@ bool stage_decide(Context* ctx, const FsWork& w)
     return true;
 }
 
+// Scan tags of a new integration (the Cartesian and polar scratch areas
+// carry them); at the wrap every area is cleared.
+bool next_epoch(Context* ctx)
+{
+    if (++ctx->epoch < 0xfff0ull) return true;
+    ctx->big_ready = false;
+    if (!ensure_big_scratch(ctx)) return false;
+    if (!ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart_bytes_of(ctx) * ctx->fs_warps,
+                                                     ctx->stream)) ||
+        !ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff,
+                                                     polar_bytes_of(ctx) * ctx->fs_warps, ctx->stream)))
+        return false;
+    ctx->epoch = 1;
+    return true;
+}
+
+// Cartesian points predicted to pass the first pass's cell budget four times
+// over or more would spend the whole budget on their warp before starting
+// again on a block after the first pass.  They run on blocks from the start
+// instead (largest first, at most kEarlyMax, with their own scratch blocks
+// after the second pass's); the first pass skips them.  Adaptive refinement
+// keeps one tape per group and does not use this path.
+bool early_routing(const Context* ctx, const FsWork& w)
+{
+    return ctx->cell_budget > 0 && w.tape == nullptr && w.early_cart != nullptr;
+}
+
+FsWork early_work(Context* ctx, const FsWork& w)
+{
+    FsWork e = w;
+    e.retry_pass = 1;
+    e.early_pass = 1;
+    e.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr) +
+                (long long)retry_blocks(ctx) * static_cast<long long>(cart_bytes_big(ctx));
+    e.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
+    e.row_cap = ctx->row_cap_big;
+    return e;
+}
+
 // Seeds of every inverse-ray point of w's work lists (at most max_points).
+// With early routing, the routed points are seeded on the early stream and
+// their block pass starts right after, beside the seeding of the others
+// (stage_integrate joins it); with stage timing on, everything stays on the
+// context's stream and stage_integrate runs the early pass first.
 bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
 {
     const int warps = ctx->fs_warps < max_points ? ctx->fs_warps : max_points;
     if (warps <= 0) return true;
+    // Early work a failed call left behind is finished before anything reuses its buffers.
+    if (ctx->early_live && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
+    if (!next_epoch(ctx)) return false;
+    ctx->early_live = false;
+    ctx->early_serial = false;
     // Candidate keys and probes share one allocation: all warps' keys, then all probes.
     const size_t per = seed_candidate_bytes_per_warp(ctx->cand_cap);
     const size_t key_bytes = per * 8 / (8 + 16);
-    char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
     cudaEvent_t ev;
+    const bool early = early_routing(ctx, w);
+    if (early) {
+        if (!ctx->check("route", launch_route_early(w, 4.0 * static_cast<double>(ctx->cell_budget),
+                                                    ctx->fs_route.ptr, max_points, ctx->sm_count, ctx->stream)))
+            return false;
+        FsWork es = w;
+        es.seed_slots = w.early_cart;
+        es.seed_count = w.ir_count + 5;
+        es.seed_next = w.next_item + 7;
+        es.seed_block_after = 0;
+        char* eb = static_cast<char*>(ctx->fs_seed_early.ptr);
+        long long* ek = reinterpret_cast<long long*>(eb);
+        P2* ep = reinterpret_cast<P2*>(eb + key_bytes * kEarlyMax);
+        if (!ctx->timing && ctx->early_stream != nullptr) {
+            if (!ctx->check("fork", cudaEventRecord(ctx->early_fork, ctx->stream)) ||
+                !ctx->check("fork", cudaStreamWaitEvent(ctx->early_stream, ctx->early_fork, 0)))
+                return false;
+            const bool ok =
+                ctx->check("seeds early", launch_seeds(es, ctx->sm_count, ctx->early_stream, ek, ep, kEarlyMax)) &&
+                ctx->check("cartesian early",
+                           launch_cartesian(early_work(ctx, w), kEarlyMax, ctx->early_stream, ctx->epoch));
+            // Recorded even after a failed launch: the context's stream must
+            // never run ahead of work already queued beside it.
+            if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream))) return false;
+            ctx->early_live = true;
+            if (!ok) return false;
+        } else {
+            ctx->stage_begin(2, &ev);
+            if (!ctx->check("seeds early", launch_seeds(es, ctx->sm_count, ctx->stream, ek, ep, kEarlyMax)))
+                return false;
+            ctx->stage_end(2, ev);
+            ctx->early_serial = true;
+        }
+        ctx->launches += 4;
+    }
+    FsWork wm = w;
+    wm.seed_skip_early = early ? 1 : 0;
+    char* cb = static_cast<char*>(ctx->fs_cand_keys.ptr);
     ctx->stage_begin(2, &ev);
-    if (!ctx->check("seeds", launch_seeds(w, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
+    if (!ctx->check("seeds", launch_seeds(wm, ctx->sm_count, ctx->stream, reinterpret_cast<long long*>(cb),
                                           reinterpret_cast<P2*>(cb + key_bytes * ctx->fs_warps), warps)))
         return false;
     // The points the one-warp pass handed over (their disks hold many
     // critical sources), one block each.
-    if (w.seed_block_after > 0 && w.retry_seeds != nullptr && w.seed_scratch != nullptr) {
-        if (!ctx->check("seeds blocks", launch_seeds_blocks(w, retry_blocks(ctx), ctx->stream))) return false;
+    if (wm.seed_block_after > 0 && wm.retry_seeds != nullptr && wm.seed_scratch != nullptr) {
+        if (!ctx->check("seeds blocks", launch_seeds_blocks(wm, retry_blocks(ctx), ctx->stream))) return false;
         ctx->launches += 1;
     }
     ctx->stage_end(2, ev);
@@ -339,52 +424,15 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
 bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
 {
     if (max_points <= 0) return true;
-    const size_t cart_bytes = cart_bytes_of(ctx);
-    const size_t pol_bytes = polar_bytes_of(ctx);
-    if (++ctx->epoch >= 0xfff0ull) {
-        ctx->big_ready = false;
-        if (!ensure_big_scratch(ctx)) return false;
-        if (!ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch.ptr, 0xff, cart_bytes * ctx->fs_warps,
-                                                         ctx->stream)) ||
-            !ctx->check("scratch reset", cudaMemsetAsync(ctx->fs_scratch_polar.ptr, 0xff,
-                                                         pol_bytes * ctx->fs_warps, ctx->stream)))
-            return false;
-        ctx->epoch = 1;
-    }
     const int warps = ctx->fs_warps < max_points ? ctx->fs_warps : max_points;
-    const bool overlap = !ctx->timing && ctx->side_stream != nullptr && ctx->early_stream != nullptr;
+    const bool overlap = !ctx->timing && ctx->side_stream != nullptr;
     cudaEvent_t ev;
-    // Cartesian points predicted to pass the first pass's cell budget four
-    // times over or more would spend the whole budget on their warp before
-    // starting again on a block.  They run on blocks from the start instead,
-    // on the early stream beside the first pass, which skips them (largest
-    // first; their own scratch blocks after the second pass's).  Adaptive
-    // refinement keeps one tape per group and does not use this path.
-    const bool early = ctx->cell_budget > 0 && w.tape == nullptr && w.early_cart != nullptr;
-    if (early) {
-        if (!ctx->check("route", launch_route_early(w, 4.0 * static_cast<double>(ctx->cell_budget),
-                                                    ctx->fs_route.ptr, max_points, ctx->sm_count, ctx->stream)))
+    if (ctx->early_serial) {
+        // Stage timing on: the early block pass (stage_seeds) runs here, first.
+        ctx->stage_begin(3, &ev);
+        if (!ctx->check("cartesian early", launch_cartesian(early_work(ctx, w), kEarlyMax, ctx->stream, ctx->epoch)))
             return false;
-        FsWork e = w;
-        e.retry_pass = 1;
-        e.early_pass = 1;
-        e.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr) +
-                    (long long)retry_blocks(ctx) * static_cast<long long>(cart_bytes_big(ctx));
-        e.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
-        e.row_cap = ctx->row_cap_big;
-        if (overlap) {
-            if (!ctx->check("fork", cudaEventRecord(ctx->early_fork, ctx->stream)) ||
-                !ctx->check("fork", cudaStreamWaitEvent(ctx->early_stream, ctx->early_fork, 0)))
-                return false;
-            const bool ok = ctx->check("cartesian early",
-                                       launch_cartesian(e, kEarlyMax, ctx->early_stream, ctx->epoch));
-            if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream)) || !ok) return false;
-        } else {
-            ctx->stage_begin(3, &ev);
-            if (!ctx->check("cartesian early", launch_cartesian(e, kEarlyMax, ctx->stream, ctx->epoch))) return false;
-            ctx->stage_end(3, ev);
-        }
-        ctx->launches += 3;
+        ctx->stage_end(3, ev);
     }
     ctx->stage_begin(3, &ev);
     if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
@@ -438,7 +486,8 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         ctx->stage_end(4, ev);
     }
     if (overlap && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0))) return false;
-    if (overlap && early && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
+    if (ctx->early_live && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
+    ctx->early_live = false;
     if (!polar_ok) return false;
     ctx->launches += 8;
     return true;
@@ -455,7 +504,8 @@ bool prepare_tables(Context* ctx, const Plan& plan)
     }
     if (!ensure_trig(ctx) || !ensure_scratch(ctx) || !ensure_big_scratch(ctx) ||
         !ctx->ensure(ctx->fs_seed_block, seed_candidate_bytes_per_warp(ctx->cand_cap) * retry_blocks(ctx)) ||
-        !ctx->ensure(ctx->fs_route, route_bytes()))
+        !ctx->ensure(ctx->fs_route, route_bytes()) ||
+        !ctx->ensure(ctx->fs_seed_early, seed_candidate_bytes_per_warp(ctx->cand_cap) * kEarlyMax))
         return false;
     const int nld = static_cast<int>(plan.ld_coeffs.size());
     if (!upload(ctx, ctx->fs_settings, plan.settings) || !upload(ctx, ctx->fs_models, plan.models) ||

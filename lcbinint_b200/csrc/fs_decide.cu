@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(128) route_estimate_kernel(FsWork w, double mi
         const int it = w.ir_cart[k];
         const FsOut o = w.out[it];
         const FsItem item = w.items[it];
-        if (o.status != kFsOk || o.n_seeds <= 0 || !(item.rho > 0.0)) continue;
+        if (o.status != kFsOk || !(item.rho > 0.0)) continue;
         const FsSettingsDev st = w.settings[item.settings];
         const double nbin = static_cast<double>(max(st.source_bins, 1));
         const double a = point_source(item.s, item.q, item.x, item.y).magnification;

@@ -508,9 +508,23 @@ __global__ void __launch_bounds__(128) seeds_kernel(FsWork w, long long* cand_ke
     const bool can_hand_over = w.seed_block_after > 0 && w.retry_seeds != nullptr;
     for (;;) {
         int k = 0;
-        if (lane_id() == 0) k = atomicAdd(&w.next_item[0], 1);
+        if (lane_id() == 0) {
+            if (w.seed_slots != nullptr) {
+                const int idx = atomicAdd(w.seed_next, 1);
+                k = idx < *w.seed_count ? w.seed_slots[idx] : total;
+            } else {
+                k = atomicAdd(&w.next_item[0], 1);
+            }
+        }
         k = shfl_i(k, 0);
         if (k >= total) break;
+        if (w.seed_skip_early && k < n_cart) {
+            // Seeded on the early stream, with the early block pass.
+            const int ne = w.ir_count[5];
+            bool routed = false;
+            for (int e = 0; e < ne; ++e) routed |= w.early_cart[e] == k;
+            if (routed) continue;
+        }
         const int it = (k < n_cart) ? w.ir_cart[k] : w.ir_polar[k - n_cart];
         const long long t_item = clock64();
         const FsItem item = w.items[it];

@@ -123,6 +123,13 @@ struct FsWork {
     // makes the block kernel take that list (work counter next_item[6]).
     int* early_cart;
     int early_pass;
+    // Seeding of a given list of Cartesian list positions (null: every point
+    // of the work lists), e.g. the early points on their own stream, with its
+    // own work counter; seed_skip_early = 1 leaves the early points out.
+    const int* seed_slots;
+    const int* seed_count;
+    int* seed_next;
+    int seed_skip_early;
 };
 
 constexpr int kEarlyMax = 32;

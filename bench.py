@@ -1039,6 +1039,8 @@ def main():
                 "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved and peak.value else None,
                 "traffic": None, "peak_source": "device-measured FP64 FMA loop (lcbi_gpu_measure_fp64_peak)",
                 "stage_ms_per_step": {k: v / stage_steps for k, v in shares.items()},
+                "achieved_over": "the dominant stage's serialised time (its passes one after another); in the timed "
+                                 "steps the passes overlap on three streams",
                 "stage_timing": f"{stage_steps} further steps, stages serialised by the per-stage events",
                 "flop_per_ray": F_RAY}
     out = {

@@ -229,7 +229,7 @@ def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
 
 
 def ps_batch_workload(n=1_000_000, seed=0):
-    """Point-source batch (config 2): y uniform in [-1.5, 1.5]^2, s log-U[0.3, 3],
+    """Point-source batch (1e6 points): y uniform in [-1.5, 1.5]^2, s log-U[0.3, 3],
     q log-U[1e-5, 1] in the core convention, per point."""
     rng = np.random.default_rng(seed)
     s = np.exp(rng.uniform(np.log(0.3), np.log(3.0), n))
@@ -243,7 +243,7 @@ LC_PARAMS = dict(t0=0.0, tE=1.0, u0=-0.01, alpha=0.5, s=0.95, q=1e-2, rho=5e-3)
 
 
 def adjoint_workload(seed=2, n_models=256, n_epochs=500):
-    """Config 4: models drawn as in config 3, epochs uniform over t0 +- 2 tE.
+    """Adjoint workload (256 models x 500 epochs): models drawn as in fs_batch, epochs uniform over t0 +- 2 tE.
     Returns params (M, 8) = (t0, tE, u0, alpha, s, q, rho, Gamma) and times (M, K)."""
     rng = np.random.default_rng(seed)
     P = np.empty((n_models, 8))
@@ -287,7 +287,7 @@ def cpu_adjoint_rate(P, T, n_procs, n_models):
 
 
 def orbital_workload(seed=3, n_models=1024, n_epochs=2000, parallax=False):
-    """Config 5, its lens-orbital-motion half: models drawn as in config 3
+    """Orbital workload, its lens-orbital-motion half: models drawn as in fs_batch
     (t0 U[-20, 20] d, tE U[10, 40] d), half of them on circular and half on
     Keplerian orbits with ds/dt / s and dalpha/dt U[-1, 1] per year and the
     line-of-sight term g3 U[0, 0.5] per year (Keplerian: lom_szs U[-0.5, 0.5],
@@ -318,12 +318,12 @@ def orbital_workload(seed=3, n_models=1024, n_epochs=2000, parallax=False):
     return dicts, modes, gams, np.linspace(-100.0, 100.0, n_epochs)
 
 
-# Sky position of the config-5 events (the Galactic bulge) for parallax.
+# Sky position of the orbital workload's events (the Galactic bulge) for parallax.
 ORBITAL_EVENT = dict(ra=268.5, dec=-29.0)
 
 
 def orbital_ephemeris():
-    """A synthetic Earth ephemeris for the parallax half of config 5 (the
+    """A synthetic Earth ephemeris for the parallax half of the orbital workload (the
     reference's table is not in its repository), named through
     LCBININT_EARTH_EPHEMERIS so that this process, the reference and the CPU
     workers read the same one."""
@@ -406,7 +406,7 @@ def cpu_ps_rate(s, q, y1, y2, n_procs, target_seconds):
 
 
 def cpu_light_curve_rate(target_seconds):
-    """The reference's own light-curve path (one curve, one core) on config 1."""
+    """The reference's own light-curve path (one curve, one core) on the README light curve."""
     from oracle.oracle import Reference, default_settings
     ref = Reference()
     times = np.linspace(-0.5, 0.5, 200)
@@ -586,7 +586,7 @@ def run_other_workload(args, world, rank, local_rank, ncores):
 
 
 def run_adjoint(args, world, rank, local_rank, ncores, common):
-    """Config 4: magnifications and their gradients in (t0, tE, u0, alpha, s,
+    """Adjoint workload: magnifications and their gradients in (t0, tE, u0, alpha, s,
     q, rho, Gamma) for 256 models x 500 epochs through the library's adjoint
     (lcbi_gpu_light_curves_grad), against the forward alone, against a plain
     GPU forward of one point per call with central finite differences (17
@@ -595,7 +595,7 @@ def run_adjoint(args, world, rank, local_rank, ncores, common):
     P, T = adjoint_workload(seed=2 + rank)
     M, K = T.shape
     n = M * K
-    config = {"workload": "adjoint: 256 models x 500 epochs (config-3 model distribution, t0 +- 2 tE), auto "
+    config = {"workload": "adjoint: 256 models x 500 epochs (fs_batch model distribution, t0 +- 2 tE), auto "
                           "decision tree, nbin 50, dA/d(t0, tE, u0, alpha, s, q, rho, Gamma)",
               "points": n, "l2": "not flushed (inputs and results under 11 MB; workspaces reused)",
               "parallelism": f"replicas x{world}"}
@@ -688,7 +688,7 @@ def run_adjoint(args, world, rank, local_rank, ncores, common):
 
 
 def run_orbital(args, world, rank, local_rank, ncores, common):
-    """Config 5: 1024 models x 2000 epochs with circular or Keplerian lens
+    """Orbital workload: 1024 models x 2000 epochs with circular or Keplerian lens
     orbital motion and annual parallax through the batched C ABI
     (lcbi_gpu_magnification_arrays, LensModel's route), host arrays in and
     out.  The Earth ephemeris is synthetic (the reference's table is not in
@@ -702,7 +702,7 @@ def run_orbital(args, world, rank, local_rank, ncores, common):
     M, K = len(dicts), times.size
     n = M * K
     config = {"workload": f"orbital: {M} models x 2000 epochs over 200 days, half circular / half Keplerian lens "
-                          "orbital motion (g1, g2 U[-1,1]/yr, g3 U[0,0.5]/yr), config-3 model distribution, "
+                          "orbital motion (g1, g2 U[-1,1]/yr, g3 U[0,0.5]/yr), fs_batch model distribution, "
                           "linear LD U[0,0.8], auto decision tree, nbin 50; " +
                           ("annual parallax piEN, piEE U[-0.5,0.5] (synthetic Earth ephemeris, event at the "
                            "Galactic bulge)" if parallax else "no parallax"),

@@ -23,7 +23,7 @@ OUT = Path(__file__).resolve().parent
 
 
 def point_source(ref: Reference):
-    """2,000 point-source magnifications, BASELINE config-2 distribution (seed 10)."""
+    """2,000 point-source magnifications, the 1e6-point batch's distribution (seed 10)."""
     rng = np.random.default_rng(10)
     n = 2000
     y = rng.uniform(-1.5, 1.5, (n, 2))

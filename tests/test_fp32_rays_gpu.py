@@ -1,5 +1,5 @@
 """FP32 ray map (lcbi_gpu_set_ray_precision(ctx, 32)) against the bit-exact
-FP64 map on forced inverse-ray points of the config-3 distribution (Cartesian
+FP64 map on forced inverse-ray points of the fs_batch distribution (Cartesian
 and polar, nbin 20-200, linear limb darkening): every magnification within
 1e-4 relative (the precision the FP32 arm is quoted at), most far closer."""
 import ctypes as C

@@ -85,7 +85,7 @@ def test_edge_cases(oracle_lib):
 
 
 def test_full_size_properties():
-    """1e6 points (the config-2 size): finite, image counts 3/5, and the
+    """1e6 points (the point-source batch size): finite, image counts 3/5, and the
     reflection symmetry A(y1, y2) == A(y1, -y2) of the binary lens."""
     import lcbinint_b200 as lb
     s, q, y1, y2 = _cfg2_points(1_000_000, 7)

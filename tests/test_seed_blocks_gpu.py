@@ -87,7 +87,7 @@ def test_block_seeding_matches_warp_seeding_and_reference(grid):
 
 
 def test_block_seeding_on_mixed_batch():
-    """A 256-point slice of the config-3 batch: every point that meets a
+    """A 256-point slice of the 4,096-point fs_batch: every point that meets a
     critical source inside its disk seeded on a block, against one warp each."""
     import bench
     from lcbinint_b200 import _lib

@@ -71,44 +71,54 @@ __device__ __forceinline__ bool angle_less(P2 l, P2 r) { return atan2(l.y, l.x) 
 __constant__ unsigned char kPermCode[24] = {228, 180, 216, 120, 156, 108, 225, 177, 201, 57, 141, 45,
                                             210, 114, 198, 54,  78,  30,  147, 99,  135, 39, 75,  27};
 
-constexpr int kTrackBatch = 64;                      // samples staged per batch
-constexpr int kTrackLoads = 4 * kTrackBatch / 32;    // points each lane loads per batch
+// Branch tracking of four models per warp, eight lanes per model: each lane
+// costs three of the 24 permutations (ranks 3g .. 3g + 2), the first least
+// cost over the model's eight lanes comes from a three-step butterfly on
+// (cost, rank), and the group's lanes share their own shuffles and barriers,
+// so the four models of a warp run independently.
+constexpr int kTrackLanes = 8;
+constexpr int kTrackPerLane = 24 / kTrackLanes;
+constexpr int kTrackGroups = 32 / kTrackLanes;
+constexpr int kTrackWarps = 4;                                  // warps per block
+constexpr int kTrackBatch = 16;                                 // steps staged per batch
+constexpr int kTrackLoads = 4 * kTrackBatch / kTrackLanes;      // points each lane loads per batch
 
-__global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models, int n_models,
-                                                          const long long* __restrict__ raw_offset,
-                                                          const P2* __restrict__ raw, P2* __restrict__ branches,
-                                                          const unsigned char* __restrict__ needed)
+__global__ void __launch_bounds__(32 * kTrackWarps) caustic_track_kernel(CausticModel* models, int n_models,
+                                                                         const long long* __restrict__ raw_offset,
+                                                                         const P2* __restrict__ raw,
+                                                                         P2* __restrict__ branches,
+                                                                         const unsigned char* __restrict__ needed)
 {
-    const int m = blockIdx.x;
-    if (m >= n_models || (needed && !needed[m])) return;
     const int lane = lane_id();
+    const int grp = lane / kTrackLanes;
+    const int g = lane % kTrackLanes;
+    const unsigned gmask = ((1u << kTrackLanes) - 1u) << (grp * kTrackLanes);
+    const int m = (blockIdx.x * kTrackWarps + warp_in_block()) * kTrackGroups + grp;
+    if (m >= n_models || (needed && !needed[m])) return;
     CausticModel md = models[m];
     const int bins = md.bins;
     const P2* pts = raw + raw_offset[m];
     P2* br = branches + md.branch_offset;
 
-    // Bounding box over every sampled point (order-independent exact min/max).
-    double mnx = dinf(), mxx = -dinf(), mny = dinf(), mxy = -dinf();
-    for (int t = lane; t < 4 * bins; t += 32) {
-        const P2 p = pts[t];
-        mnx = dmin_(mnx, p.x);
-        mxx = dmax_(mxx, p.x);
-        mny = dmin_(mny, p.y);
-        mxy = dmax_(mxy, p.y);
+    // The permutations this lane costs.
+    int perm[kTrackPerLane][4];
+    unsigned code_of[kTrackPerLane];
+#pragma unroll
+    for (int j = 0; j < kTrackPerLane; ++j) {
+        perm_of_rank(g * kTrackPerLane + j, perm[j]);
+        code_of[j] = kPermCode[g * kTrackPerLane + j];
     }
-    mnx = warp_min(mnx);
-    mxx = warp_max(mxx);
-    mny = warp_min(mny);
-    mxy = warp_max(mxy);
 
     // Branch tracking: sample 0 sorted by polar angle, then each sample assigned
     // by the first minimum-cost permutation in lexicographic order.
-    int perm[4];
-    perm_of_rank(lane < 24 ? lane : 0, perm);
-    const unsigned my_code = kPermCode[lane < 24 ? lane : 0];
     P2 end[4];
+    double mnx, mxx, mny, mxy;
     {
         P2 v[4] = {pts[0], pts[1], pts[2], pts[3]};
+        mnx = dmin_(dmin_(v[0].x, v[1].x), dmin_(v[2].x, v[3].x));
+        mxx = dmax_(dmax_(v[0].x, v[1].x), dmax_(v[2].x, v[3].x));
+        mny = dmin_(dmin_(v[0].y, v[1].y), dmin_(v[2].y, v[3].y));
+        mxy = dmax_(dmax_(v[0].y, v[1].y), dmax_(v[2].y, v[3].y));
         for (int i = 1; i < 4; ++i) {
             const P2 x = v[i];
             int k = i;
@@ -120,67 +130,90 @@ __global__ void __launch_bounds__(32) caustic_track_kernel(CausticModel* models,
         }
 #pragma unroll
         for (int b = 0; b < 4; ++b) end[b] = v[b];
-        if (lane < 4) br[(long long)lane * bins] = v[lane];
+        if (g < 4) br[(long long)g * bins] = v[g];
     }
     // The samples are consumed strictly in order, one step (4 points) at a
     // time, and each step's assignment depends on the previous one; so the
     // points are staged in shared memory kTrackBatch steps at a time, the
     // next batch being loaded into registers while the current one is
-    // consumed, which keeps the memory latency off the serial chain.
-    __shared__ P2 stage[4 * kTrackBatch];
+    // consumed.  The loads also give the bounding box over every sampled
+    // point (exact min/max, independent of the order).
+    __shared__ P2 stage_all[kTrackWarps][kTrackGroups][4 * kTrackBatch];
+    P2* stage = stage_all[warp_in_block()][grp];
     P2 nxt[kTrackLoads];
     auto load_batch = [&](int s0) {
         const long long first = 4ll * s0, last = 4ll * bins;
 #pragma unroll
         for (int u = 0; u < kTrackLoads; ++u) {
-            const long long j = first + lane + 32 * u;
-            if (j < last) nxt[u] = pts[j];
+            const long long j = first + g + kTrackLanes * u;
+            if (j < last) {
+                nxt[u] = pts[j];
+                mnx = dmin_(mnx, nxt[u].x);
+                mxx = dmax_(mxx, nxt[u].x);
+                mny = dmin_(mny, nxt[u].y);
+                mxy = dmax_(mxy, nxt[u].y);
+            }
         }
     };
     double max_seg2 = 0.0;
     load_batch(1);
     for (int s0 = 1; s0 < bins; s0 += kTrackBatch) {
         const int s1 = min(bins, s0 + kTrackBatch);
-        __syncwarp();
+        __syncwarp(gmask);
 #pragma unroll
         for (int u = 0; u < kTrackLoads; ++u) {
-            const int j = lane + 32 * u;
+            const int j = g + kTrackLanes * u;
             if (j < 4 * (s1 - s0)) stage[j] = nxt[u];
         }
-        __syncwarp();
+        __syncwarp(gmask);
         if (s1 < bins) load_batch(s1);
-    for (int i = s0; i < s1; ++i) {
-        const P2* cur = stage + 4 * (i - s0);
-        double cost = 0.0;
+        for (int i = s0; i < s1; ++i) {
+            const P2* cur = stage + 4 * (i - s0);
+            // This lane's first least cost; a cost that is not below +inf (NaN
+            // included) competes as +inf, so with none below +inf rank 0 wins,
+            // as in a serial scan with a strict comparison.
+            double best = dinf();
+            int bp = 64;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) cost += dist2(end[b], cur[perm[b]]);
-        // The first permutation of least cost: a butterfly over (cost, rank),
-        // ties going to the lower rank; a cost that is not below +inf (NaN
-        // included) never wins, and with none below +inf rank 0 does, as in a
-        // serial scan with a strict comparison.
-        double best = (lane < 24 && cost < dinf()) ? cost : dinf();
-        int bp = lane < 24 ? lane : 32 + lane;
+            for (int j = 0; j < kTrackPerLane; ++j) {
+                double cost = 0.0;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-            const int op = __shfl_xor_sync(0xffffffffu, bp, off);
-            if (ob < best || (ob == best && op < bp)) {
-                best = ob;
-                bp = op;
+                for (int b = 0; b < 4; ++b) cost += dist2(end[b], cur[perm[j][b]]);
+                const double c = cost < dinf() ? cost : dinf();
+                const int r = g * kTrackPerLane + j;
+                if (c < best || (c == best && r < bp)) {
+                    best = c;
+                    bp = r;
+                }
             }
-        }
-        const unsigned code = __shfl_sync(0xffffffffu, my_code, bp);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const P2 sel = cur[(code >> (2 * b)) & 3u];
-            const double seg2 = dist2(end[b], sel);
-            if (seg2 > max_seg2) max_seg2 = seg2;
-            end[b] = sel;
+            for (int off = kTrackLanes / 2; off > 0; off >>= 1) {
+                const double ob = __shfl_xor_sync(gmask, best, off);
+                const int op = __shfl_xor_sync(gmask, bp, off);
+                if (ob < best || (ob == best && op < bp)) {
+                    best = ob;
+                    bp = op;
+                }
+            }
+            const unsigned code = kPermCode[bp];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const P2 sel = cur[(code >> (2 * b)) & 3u];
+                const double seg2 = dist2(end[b], sel);
+                if (seg2 > max_seg2) max_seg2 = seg2;
+                end[b] = sel;
+            }
+            if (g < 4) br[(long long)g * bins + i] = cur[(code >> (2 * g)) & 3u];
         }
-        if (lane < 4) br[(long long)lane * bins + i] = cur[(code >> (2 * lane)) & 3u];
     }
+#pragma unroll
+    for (int off = kTrackLanes / 2; off > 0; off >>= 1) {
+        mnx = dmin_(mnx, __shfl_xor_sync(gmask, mnx, off));
+        mxx = dmax_(mxx, __shfl_xor_sync(gmask, mxx, off));
+        mny = dmin_(mny, __shfl_xor_sync(gmask, mny, off));
+        mxy = dmax_(mxy, __shfl_xor_sync(gmask, mxy, off));
     }
-    if (lane == 0) {
+    if (g == 0) {
         md.min_x = mnx;
         md.max_x = mxx;
         md.min_y = mny;
@@ -212,7 +245,9 @@ cudaError_t launch_caustics(CausticModel* models, int n_models, int max_bins, co
                                                    critical_points ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    caustic_track_kernel<<<n_models, 32, 0, stream>>>(models, n_models, raw_offset, raw, branches, needed);
+    const int per_block = kTrackWarps * kTrackGroups;
+    caustic_track_kernel<<<(n_models + per_block - 1) / per_block, 32 * kTrackWarps, 0, stream>>>(
+        models, n_models, raw_offset, raw, branches, needed);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,6 @@ struct CartShared {
     double x[32 * W];   // abscissa of each chunk cell
     unsigned in[W];     // inside masks
     unsigned cont[W];   // left scan: abscissa >= xmin(previous row) - dx
-    double sum;         // broadcast of a sequential brightness sum
     int item;
     int red[W];
 };
@@ -276,23 +275,15 @@ __device__ __forceinline__ int first_event(const CartShared<W>& S, int from, boo
     return Grp<W>::N;
 }
 
-// Sequential brightness sum of chunk cells [a, b) in order, in every thread.
+// Sequential brightness sum of chunk cells [a, b) in order.  Every thread
+// forms the same sum from broadcast reads, so no barrier is needed to share
+// it (one thread summing while the others waited at two barriers measured
+// about 1 % slower on a 200-epoch light curve).
 template <int W>
 __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a, int b)
 {
-    if (W == 1) {
-        for (int j = a; j < b; ++j) acc += S.b[j];
-        return acc;
-    }
-    if (threadIdx.x == 0) {
-        double v = acc;
-        for (int j = a; j < b; ++j) v += S.b[j];
-        S.sum = v;
-    }
-    __syncthreads();
-    const double r = S.sum;
-    __syncthreads();
-    return r;
+    for (int j = a; j < b; ++j) acc += S.b[j];
+    return acc;
 }
 
 // cartesian_image_area_impl: one directional flood fill from `seed`.

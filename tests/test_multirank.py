@@ -34,7 +34,8 @@ def _rank_main(rank, world, port, out):
 def test_replica_reduction_over_two_gloo_ranks():
     import torch.multiprocessing as mp
     port = _free_port()
-    with mp.Manager() as m:
+    # spawn, not fork: the test process may already hold a CUDA context
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)

@@ -116,6 +116,74 @@ def fs_settings_for(rows):
     return settings, idx
 
 
+def fs_batch_arrays(rows):
+    """The C-ABI inputs of a forced inverse-ray batch: the settings list (one
+    entry per distinct (Gamma, grid, nbin)), the distinct lens models and the
+    FS_POINT_DTYPE records that index them."""
+    from lcbinint_b200.api import FS_POINT_DTYPE, PS_EXACT, PS_ON_DEVICE
+    settings, sidx = fs_settings_for(rows)
+    mkeys = {}
+    mlist = []
+    midx = np.empty(len(rows), dtype=np.int32)
+    for i, r in enumerate(rows):
+        k = (r[0], r[1])
+        if k not in mkeys:
+            mkeys[k] = len(mlist)
+            mlist.append((r[0], r[1], 1400, 0))
+        midx[i] = mkeys[k]
+    models = np.array(mlist, dtype=np.dtype([("s", "f8"), ("q", "f8"), ("bins", "i4"), ("r", "i4")]))
+    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
+    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
+    pts["settings"] = sidx
+    pts["model"] = midx
+    pts["flags"] = PS_EXACT | PS_ON_DEVICE
+    return settings, models, pts
+
+
+def reference_inverse_ray(rows, n_procs):
+    """The reference's binary_inverse_ray on every row, one process per core
+    (its solver keeps static state, so never threads); returns the
+    magnifications and methods in row order and the pool's wall time."""
+    import multiprocessing as mp
+    n_procs = max(1, min(n_procs, len(rows)))
+    chunks = [(rows[k::n_procs],) for k in range(n_procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n_procs) as pool:
+        pool.map(_ref_worker, [(rows[:1],)] * n_procs)  # imports and library loads
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, chunks)
+        wall = time.perf_counter() - t0
+    A = np.empty(len(rows))
+    M = np.empty(len(rows), dtype=np.int32)
+    for k, (_, out, meth) in enumerate(res):
+        A[k::n_procs] = out
+        M[k::n_procs] = meth
+    return A, M, wall
+
+
+def parity_summary(A, method, status, R, RM):
+    """Agreement of the device's results with the reference's on the same
+    points: Cartesian magnifications bit for bit, polar ones (same cells, an
+    exact sum instead of a running one) to 1e-12 relative, methods equal."""
+    cart = method == 2
+    pol = method == 3
+    same_bits = A.view(np.int64) == R.view(np.int64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(same_bits, 0.0, np.abs(A / R - 1.0))
+    rel = np.where(np.isfinite(rel), rel, np.inf)
+    return {
+        "vs": "the reference compiled from its sources (oracle/_ref), binary_inverse_ray on the same points",
+        "points": int(A.size), "bit_exact": int(same_bits.sum()),
+        "cartesian": {"points": int(cart.sum()), "bit_exact": int(same_bits[cart].sum())},
+        "polar": {"points": int(pol.sum()), "bit_exact": int(same_bits[pol].sum()),
+                  "max_rel": float(rel[pol].max()) if pol.any() else 0.0},
+        "max_rel": float(rel.max()) if rel.size else 0.0,
+        "methods_equal": int((method == RM).sum()), "status_ok": int((status == 0).sum()),
+        "pass": bool(same_bits[cart].all() and (rel[pol] <= 1e-12).all() and (method == RM).all()
+                     and (status == 0).all()),
+    }
+
+
 # --------------------------------------------------------------------------- helpers
 
 class ClockSampler:
@@ -191,11 +259,13 @@ def _ref_worker(args):
     ref = Reference()
     t = time.perf_counter()
     out = []
+    meth = []
     for r in rows:
         st = default_settings(source_bins=int(r[7]), finite_mode=int(r[6]), limb_darkening_c=float(r[5]))
-        A, _ = ref.inverse_ray(st, r[0], r[1], r[2], r[3], r[4])
+        A, m = ref.inverse_ray(st, r[0], r[1], r[2], r[3], r[4])
         out.append(A[0])
-    return time.perf_counter() - t, out
+        meth.append(int(m[0]))
+    return time.perf_counter() - t, out, meth
 
 
 def cpu_reference_rate(rows, n_procs, target_seconds=20.0, seed=7):
@@ -858,7 +928,7 @@ def main():
     config = {"workload": "fs_batch: 4096 forced inverse-ray points, 64 models x 64 epochs, "
                           "Cartesian/polar mixed, nbin 20-200, linear LD",
               "points": int(len(rows)), "models": 64,
-              "precision": "fp64 (bit-exact vs reference)" if args.rays == "f64" else
+              "precision": "fp64" if args.rays == "f64" else
                            "fp32 ray map about image-centred anchors, fp64 sums, fp64 seeds and decisions",
               "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
 
@@ -867,7 +937,7 @@ def main():
             return
         per_step = []
         for _ in range(args.warmup + args.steps):
-            rate, n, wall = cpu_reference_rate(rows, ncores, target_seconds=max(2.0, args.cpu_seconds / 4))
+            rate, n, wall = cpu_reference_rate(rows, ncores, target_seconds=max(2.0, args.cpu_seconds / 4))[:3]
             per_step.append((rate, n, wall))
         timed = per_step[args.warmup:]
         tot_n = sum(x[1] for x in timed)
@@ -894,7 +964,7 @@ def main():
 
     import lcbinint_b200 as lb
     from lcbinint_b200 import _lib
-    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, PS_EXACT, PS_ON_DEVICE, LcbiStructs
+    from lcbinint_b200.api import FS_RESULT_DTYPE, LcbiStructs
 
     ctx = lb.context(local_rank)
     L = ctx._L
@@ -904,24 +974,8 @@ def main():
         ctx.check(L.lcbi_gpu_set_cell_budget(ctx.handle, 1), "lcbi_gpu_set_cell_budget")
         ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 2, 16384), "lcbi_gpu_set_workspace")
 
-    settings, sidx = fs_settings_for(rows)
+    settings, models, pts = fs_batch_arrays(rows)
     st_arr = (LcbiStructs.FsSettings * len(settings))(*settings)
-    # models: distinct (s, q_core)
-    mkeys = {}
-    mlist = []
-    midx = np.empty(len(rows), dtype=np.int32)
-    for i, r in enumerate(rows):
-        k = (r[0], r[1])
-        if k not in mkeys:
-            mkeys[k] = len(mlist)
-            mlist.append((r[0], r[1], 1400, 0))
-        midx[i] = mkeys[k]
-    models = np.array(mlist, dtype=np.dtype([("s", "f8"), ("q", "f8"), ("bins", "i4"), ("r", "i4")]))
-    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
-    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
-    pts["settings"] = sidx
-    pts["model"] = midx
-    pts["flags"] = PS_EXACT | PS_ON_DEVICE
     n = len(pts)
     d_pts = torch.from_numpy(pts.view(np.uint8).copy()).to(dev)
     d_res = torch.zeros(n * FS_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
@@ -1059,9 +1113,18 @@ def main():
     if fp32_error is not None:
         out["fp32_error"] = fp32_error
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        rate, nn, wall = cpu_reference_rate(rows, ncores, target_seconds=args.cpu_seconds)
-        out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",
-                               "sample": f"{nn} random points of the batch, {wall:.1f} s wall on {ncores} processes"}
+        # The reference on every point of the batch: its rate is the CPU
+        # baseline, and its magnifications are the parity check of this run.
+        R, RM, wall = reference_inverse_ray(rows, ncores)
+        out["cpu_baseline"] = {"value": len(rows) / wall, "unit": "magnifications/s", "cores": ncores,
+                               "kind": "reference",
+                               "sample": f"all {len(rows)} points of the batch, {wall:.1f} s wall on {ncores} "
+                                         "processes"}
+        if args.rays == "f64":
+            out["parity"] = parity_summary(res["magnification"].copy(), res["method"].copy(),
+                                           res["status"].copy(), R, RM)
+            if out["parity"]["pass"]:
+                config["precision"] = "fp64, bit-exact vs reference (see parity)"
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:

@@ -47,6 +47,14 @@ void lcbi_gpu_destroy(lcbi_gpu_context *ctx);
 const char *lcbi_gpu_last_error(const lcbi_gpu_context *ctx);
 /* Number of kernels this context has launched (instrumentation). */
 int64_t lcbi_gpu_launch_count(const lcbi_gpu_context *ctx);
+/* Device bytes the context's workspaces hold now (they grow with the batches
+ * and are kept for the next call; no reference counterpart). */
+int64_t lcbi_gpu_workspace_bytes(lcbi_gpu_context *ctx);
+/* The compute capability the library's device code was built for, as the
+ * driver reports it for the current device (cudaFuncAttributes::binaryVersion,
+ * 100 for sm_100a); LCBI_GPU_ERROR when no device can run it.  No reference
+ * counterpart. */
+int lcbi_gpu_kernel_binary_version(int32_t *version);
 /* Runs the context's work on a caller's cudaStream_t (NULL: the context's own
  * stream), so callers can order and time it with their own events. */
 int lcbi_gpu_set_stream(lcbi_gpu_context *ctx, void *cuda_stream);
@@ -126,6 +134,20 @@ int lcbi_gpu_binary_mag0(lcbi_gpu_context *ctx, int64_t n, const double *s, cons
 int lcbi_gpu_binary_images_mag(lcbi_gpu_context *ctx, int64_t n, const double *s, const double *q,
                                const double *y1, const double *y2, double *A, int32_t *image_count,
                                unsigned flags);
+
+/* The five image candidates of PointSourceMagnifier::binary_image_candidates
+ * (src/lcbinint/magnification/point_source_magnifier.cpp:739-778), sorted by
+ * residual, for n source positions (the conventions of lcbi_gpu_binary_mag0).
+ * candidates[20 i + 4 k ...] = {x, y, jacobian determinant, sqrt residual} of
+ * candidate k of position i, in the frame of the lens-equation roots;
+ * n_physical[i] = how many lead the list as physical images (3 or 5;
+ * PointSourceMagnifier::binary_images keeps those).  n_physical[i] = 0 (and
+ * position i's records untouched) when s == 0 or q <= 0, where the reference
+ * returns no candidate; -1 when the source sits exactly on the lighter lens,
+ * where the reference's solver does not terminate. */
+int lcbi_gpu_binary_image_candidates(lcbi_gpu_context *ctx, int64_t n, const double *s, const double *q,
+                                     const double *y1, const double *y2, double *candidates,
+                                     int32_t *n_physical, unsigned flags);
 
 /* Point-source magnification plus the smoothness indicator the finite-source
  * decision tree uses.  Replaces PointSourceMagnifier::binary_mag0_with_derivatives
@@ -295,6 +317,12 @@ int lcbi_gpu_binary_geometry(lcbi_gpu_context *ctx, double s, double q, int32_t 
  * cells whose centre maps inside the source disk), for ray-throughput
  * accounting; no reference counterpart.  n must not exceed that call's size. */
 int lcbi_gpu_last_ray_counts(lcbi_gpu_context *ctx, int64_t n, uint64_t *rays);
+
+/* FiniteSourceResult::refinement_level of each point of the last
+ * finite-source call (finite_source_magnifier.hpp:58; 0 unless the point was
+ * refined adaptively or scanned again at twice the bins).  n must not exceed
+ * that call's size. */
+int lcbi_gpu_last_refinement_levels(lcbi_gpu_context *ctx, int64_t n, int32_t *levels);
 
 /* Finite-source magnification that allocates nothing.  No reference
  * counterpart: the reference allocates freely on the host, and the entry
@@ -475,6 +503,16 @@ int lcbi_circular_orbital_motion(double time, double separation, double angle, d
                                  double reference_time, double *state);
 int lcbi_kepler_orbital_motion(double time, double separation, double angle, double g1, double g2, double g3,
                                double szs, double ar, double reference_time, double *state);
+
+/* LightCurve.source_trajectory (python/lcbinint_pybind.cpp:3292-3330 over
+ * PyLightCurveEvaluator::dynamic_source_trajectory, :1819-1880): the source
+ * position in the lens frame at each of n times, x[i], y[i].  The straight
+ * line in the options' coordinates, moved by annual (and terrestrial) parallax
+ * when piEN or piEE is non-zero, and turned into the frame of the binary's
+ * axis at that time under lens orbital motion.  Host arithmetic, bit-identical
+ * to the reference's.  options NULL means the defaults. */
+int lcbi_source_trajectory(const lcbi_params *params, const lcbi_options *options, const double *times, int64_t n,
+                           double *x, double *y);
 
 /* The Earth ephemeris for annual parallax (no counterpart in the reference's
  * ABI: the reference reads the file named by the LCBININT_EARTH_EPHEMERIS

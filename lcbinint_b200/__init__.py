@@ -11,7 +11,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import GpuError, LibraryMissing, context
-from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, GeometryBranches, LightCurve, LightCurveFunc,
+from .api import (CIRCULAR, KEPLER, STATIC, EventCoordinates, GeometryBranches, GeometryCurve, LightCurve,
+                  LightCurveFunc,
                   LightCurveInfo, LimbDarkening, Options, binary_geometry, binary_inverse_ray,
                   binary_inverse_ray_batch, binary_mag, circular_orbital_motion, kepler_orbital_motion, light_curves,
                   magnification_arrays, set_earth_ephemeris)
@@ -26,6 +27,7 @@ __all__ = [
     "magnification_arrays",
     "binary_geometry",
     "GeometryBranches",
+    "GeometryCurve",
     "circular_orbital_motion",
     "kepler_orbital_motion",
     "set_earth_ephemeris",

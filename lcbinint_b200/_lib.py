@@ -158,6 +158,16 @@ def _declare(L):
     L.lcbi_circular_orbital_motion.restype = C.c_int
     L.lcbi_kepler_orbital_motion.argtypes = [C.c_double] * 9 + [_vp]
     L.lcbi_kepler_orbital_motion.restype = C.c_int
+    L.lcbi_gpu_binary_image_candidates.argtypes = [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, C.c_uint]
+    L.lcbi_gpu_binary_image_candidates.restype = C.c_int
+    L.lcbi_gpu_last_refinement_levels.argtypes = [_vp, C.c_int64, _vp]
+    L.lcbi_gpu_last_refinement_levels.restype = C.c_int
+    L.lcbi_gpu_workspace_bytes.argtypes = [_vp]
+    L.lcbi_gpu_workspace_bytes.restype = C.c_int64
+    L.lcbi_gpu_kernel_binary_version.argtypes = [_vp]
+    L.lcbi_gpu_kernel_binary_version.restype = C.c_int
+    L.lcbi_source_trajectory.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
+    L.lcbi_source_trajectory.restype = C.c_int
 
 
 def exported_symbols() -> list[str]:

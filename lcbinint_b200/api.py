@@ -389,6 +389,14 @@ class GeometryBranches:
     y: list = field(default_factory=list)
 
 
+@dataclass
+class GeometryCurve:
+    """lcbinint.GeometryCurve (PYB:45-49, 2806-2809): a source trajectory."""
+    times: list = field(default_factory=list)
+    x: list = field(default_factory=list)
+    y: list = field(default_factory=list)
+
+
 def binary_geometry(s: float, q_core: float, n_points: int, caustic: bool, *, device: int = 0) -> GeometryBranches:
     """Caustic or critical-curve branches of a binary lens (lcbi_gpu_binary_geometry)."""
     if int(n_points) < 8:
@@ -620,6 +628,39 @@ class LightCurve:
         q = g["q"]
         q_core = 1.0 / q if (self.options.vbm_compatible and q != 0.0) else q
         return binary_geometry(separation, q_core, int(g["n_points"]), caustic)
+
+    _TRAJECTORY_KEYWORDS = ("t0", "tE", "u0", "alpha", "s", "q", "piEN", "piEE", "g1", "g2", "g3", "lom_szs",
+                            "lom_ar")
+
+    def source_trajectory(self, times, params=None, **kw) -> GeometryCurve:
+        """LightCurve.source_trajectory (PYB:3292-3330): the source position in the
+        lens frame at each time (lcbi_source_trajectory).  A dictionary's
+        piEN/piEE always count (PYB:2529-2537); as keywords they need
+        LightCurve(parallax=True) (PYB:2580-2600)."""
+        times = np.ascontiguousarray(times, dtype=np.float64).ravel()
+        if params is not None:
+            if kw:
+                raise TypeError("pass the parameters either as a dictionary or as keywords")
+            p = dict(params)
+        else:
+            unknown = set(kw) - set(self._TRAJECTORY_KEYWORDS)
+            if unknown:
+                raise TypeError(f"unexpected keyword arguments: {sorted(unknown)}")
+            if ("piEN" in kw or "piEE" in kw) and not self.parallax:
+                raise ValueError("piEN/piEE require LightCurve(parallax=True); the current trajectory model is static")
+            p = dict(kw)
+        p["rho"] = 0.0
+        cp = binary_c_params([p], self.limb_darkening, self.event, self.orbital_motion_mode, parallax=True,
+                             terrestrial_parallax=True)
+        co = self.options.c_options()
+        x = np.empty(times.size)
+        y = np.empty(times.size)
+        L = _lib.lib()
+        rc = L.lcbi_source_trajectory(_lib.ptr(cp), _lib.ptr(co), _lib.ptr(times), times.size, _lib.ptr(x),
+                                      _lib.ptr(y))
+        if rc != _lib.LCBI_OK:
+            raise ValueError("invalid argument")
+        return GeometryCurve(times=times.tolist(), x=x.tolist(), y=y.tolist())
 
     def caustics(self, params=None, n_points=None, **kw):
         """LightCurve.caustics (PYB:1525-1542, 2539-2556): four tracked caustic branches."""

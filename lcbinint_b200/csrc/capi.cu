@@ -300,6 +300,27 @@ int64_t lcbi_gpu_launch_count(const lcbi_gpu_context* c)
     return c ? reinterpret_cast<const Context*>(c)->launches : 0;
 }
 
+int lcbi_gpu_kernel_binary_version(int32_t* version)
+{
+    if (!version) return LCBI_INVALID_ARGUMENT;
+    int v = 0;
+    if (lcbi::kernel_binary_version(&v) != cudaSuccess) {
+        cudaGetLastError();
+        return LCBI_GPU_ERROR;
+    }
+    *version = v;
+    return LCBI_OK;
+}
+
+int64_t lcbi_gpu_workspace_bytes(lcbi_gpu_context* c)
+{
+    if (!c) return -1;
+    Context* ctx = reinterpret_cast<Context*>(c);
+    int64_t total = 0;
+    for (const lcbi::Buffer* b : ctx->all_buffers()) total += static_cast<int64_t>(b->bytes);
+    return total;
+}
+
 int lcbi_gpu_binary_mag0(lcbi_gpu_context* c, int64_t n, const double* s, const double* q, const double* y1,
                          const double* y2, double* A, int32_t* image_count, int32_t* status, unsigned flags)
 {
@@ -358,6 +379,37 @@ int lcbi_gpu_binary_images_mag(lcbi_gpu_context* c, int64_t n, const double* s, 
     ctx->launches += 1;
     if (!ctx->copy_back(A, dA, N, dev) || !ctx->copy_back(reinterpret_cast<int*>(image_count), dn, N, dev) ||
         !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_binary_image_candidates(lcbi_gpu_context* c, int64_t n, const double* s, const double* q,
+                                     const double* y1, const double* y2, double* candidates, int32_t* n_physical,
+                                     unsigned flags)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (!s || !q || !y1 || !y2 || !candidates || !n_physical) return LCBI_INVALID_ARGUMENT;
+    ctx->error.clear();
+    cudaSetDevice(ctx->device);
+    const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
+    const size_t N = static_cast<size_t>(n);
+    const double *ds, *dq, *dy1, *dy2;
+    double* dcand;
+    int* dn;
+    if (!ctx->stage_in(ctx->in[0], s, N, dev, &ds) || !ctx->stage_in(ctx->in[1], q, N, dev, &dq) ||
+        !ctx->stage_in(ctx->in[2], y1, N, dev, &dy1) || !ctx->stage_in(ctx->in[3], y2, N, dev, &dy2) ||
+        !ctx->stage_out(ctx->out[0], candidates, 20 * N, dev, &dcand) ||
+        !ctx->stage_out(ctx->out[1], reinterpret_cast<int*>(n_physical), N, dev, &dn))
+        return LCBI_GPU_ERROR;
+    if (!ctx->check("ps_candidates_kernel",
+                    lcbi::launch_ps_candidates(ds, dq, dy1, dy2, reinterpret_cast<double4*>(dcand), dn, n,
+                                               ctx->sm_count, ctx->stream)))
+        return LCBI_GPU_ERROR;
+    ctx->launches += 1;
+    if (!ctx->copy_back(candidates, dcand, 20 * N, dev) ||
+        !ctx->copy_back(reinterpret_cast<int*>(n_physical), dn, N, dev) || !ctx->finish())
         return LCBI_GPU_ERROR;
     return LCBI_OK;
 }

@@ -529,6 +529,60 @@ int lcbi_gpu_magnification_arrays(lcbi_gpu_context* ctx, int32_t n_sets, const l
     return LCBI_OK;
 }
 
+int lcbi_source_trajectory(const lcbi_params* params, const lcbi_options* options, const double* times, int64_t n,
+                           double* x, double* y)
+{
+    if (!params || n < 0 || (n > 0 && (!times || !x || !y))) return LCBI_INVALID_ARGUMENT;
+    const lcbi_params& p = *params;
+    const lcbi_options o = options ? *options : lcbi_default_options();
+    const bool vbm = o.vbm_compatible != 0;
+    // Only parallax moves the source off the straight line here; the
+    // trajectory applies no xallarap on this route (trajectory.hpp:12-13).
+    const bool parallax = p.piEN != 0.0 || p.piEE != 0.0;
+    const lcbi::Trajectory traj = parallax ? lcbi::make_trajectory(p) : lcbi::Trajectory{};
+    const double cos_t = std::cos(p.theta);
+    const double sin_t = std::sin(p.theta);
+    for (int64_t i = 0; i < n; ++i) {
+        double sx, sy;
+        if (!parallax) {
+            const double tau = (times[i] - p.t0) / p.tE;
+            const double beta = p.umin;
+            if (vbm) {
+                sx = tau * cos_t - beta * sin_t;
+                sy = tau * sin_t + beta * cos_t;
+            } else {
+                sx = beta * sin_t + tau * cos_t;
+                sy = beta * cos_t - tau * sin_t;
+            }
+        } else {
+            lcbi::source_position(traj, times[i], vbm, LCBI_XALLARAP_NONE, &sx, &sy);
+        }
+        if (p.orbital_motion_mode != LCBI_ORBIT_STATIC) {
+            const Orbit orb = orbit_at(p, times[i]);
+            if (vbm) {
+                // (tau, beta) are taken back out of the trajectory point and
+                // turned by the orbit's angle.
+                const double tau = sx * cos_t + sy * sin_t;
+                const double beta = -sx * sin_t + sy * cos_t;
+                const double nx = tau * std::cos(orb.angle) - beta * std::sin(orb.angle);
+                const double ny = beta * std::cos(orb.angle) + tau * std::sin(orb.angle);
+                sx = nx;
+                sy = ny;
+            } else {
+                const double c = std::cos(orb.angle - p.theta);
+                const double s = std::sin(orb.angle - p.theta);
+                const double rx = sx * c + sy * s;
+                const double ry = sy * c - sx * s;
+                sx = rx;
+                sy = ry;
+            }
+        }
+        x[i] = sx;
+        y[i] = sy;
+    }
+    return LCBI_OK;
+}
+
 lcbi_status lcbi_magnification(double time, const lcbi_params* params, const lcbi_options* options,
                                lcbi_result* result)
 {

@@ -1300,4 +1300,18 @@ int lcbi_gpu_last_ray_counts(lcbi_gpu_context* c, int64_t n, uint64_t* rays)
     return LCBI_OK;
 }
 
+int lcbi_gpu_last_refinement_levels(lcbi_gpu_context* c, int64_t n, int32_t* levels)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !levels || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (n == 0) return LCBI_OK;
+    if (ctx->fs_levels.ptr == nullptr || (size_t)n * sizeof(int32_t) > ctx->fs_levels.bytes)
+        return LCBI_INVALID_ARGUMENT;
+    if (!ctx->check("levels D2H", cudaMemcpyAsync(levels, ctx->fs_levels.ptr, n * sizeof(int32_t),
+                                                  cudaMemcpyDeviceToHost, ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
 } // extern "C"

@@ -221,10 +221,12 @@ typedef struct lcbi_fs_result {
 #define LCBI_GPU_LIMIT_SEEDS 17
 #define LCBI_GPU_LIMIT_ROWS 18
 #define LCBI_GPU_LIMIT_QUEUE 19
-/* Adaptive refinement of a point that the reference would first scan again
- * at twice the bins (needs_global_topology_retry, finite_source_magnifier.cpp:
- * 1108-1121: fewer than 50 bins, at least 16 seeds, 100 overlaps, 1,000 gap
- * repairs and a 1,000-cell jump): that rerun is not built. */
+/* No longer returned: a point that meets needs_global_topology_retry
+ * (finite_source_magnifier.cpp:1108-1121: adaptive_source_bins set, fewer than
+ * 50 bins, rho < 1e-2, at least 16 seeds, 100 overlaps, 1,000 gap repairs and
+ * a 1,000-cell jump) is scanned again at min(max_source_bins, max(50, 2 nbin))
+ * bins as the reference does (:3168-3196), refinement level 1.  The value
+ * stays reserved. */
 #define LCBI_GPU_TOPOLOGY_RETRY 21
 
 #define LCBI_GPU_MODELS_GIVEN 2u  /* points carry model indices into `models` */

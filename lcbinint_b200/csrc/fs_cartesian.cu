@@ -625,11 +625,14 @@ struct Refined {
 };
 
 // The refinement loop (FSM:3201-3280) over the tape, by one thread; the heap
-// lives in `heap` (capacity `cap` cells).  `err0` is the scan's error estimate.
+// lives in `heap` (capacity `cap` cells).  `err0` is the scan's error
+// estimate, `level0` the refinement level before the loop (1 after a
+// topology retry).
 __device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, double err0, double scale, int active_bins,
+                          int level0,
                           RefCell* heap, int cap)
 {
-    Refined out{A, err0, 0, false};
+    Refined out{A, err0, level0, false};
     const double safety =
         st.source_bins < 32 ? 8.0 : (C.rho >= 8.0e-3 ? 2.5 : (C.rho >= 3.0e-3 ? 1.8 : 1.25));
     auto guarded = [&](double mag) { return (st.tol + st.reltol * dmax_(fabs(mag), 1.0)) / safety; };
@@ -650,7 +653,7 @@ __device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, doubl
     int max_depth = 0;
     for (int bins = active_bins > 1 ? active_bins : 1; bins < max_bins && max_depth < 8; bins *= 2) ++max_depth;
     const int max_splits = 4 * max_bins > 64 ? 4 * max_bins : 64;
-    int splits = 0, level = 0;
+    int splits = 0, level = level0;
     while (n > 0 && lerr > guarded(A + corr / scale) * scale && splits < max_splits) {
         RefCell parent = heap_pop(heap, n);
         if (parent.err <= 0.0 || parent.depth >= max_depth) break;
@@ -711,6 +714,166 @@ __device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, doubl
     out.err = e;
     out.level = level;
     return out;
+}
+
+// One scan of a point's lattice (inverse_ray_cartesian_binary_mag,
+// FSM:2470-2768) at `source_bins` cells per source radius: the directional
+// flood fills of every seed that no earlier seed's rows cover, their gap
+// repairs and the overlap bookkeeping between seeds.  Leaves the summed
+// brightness in `area` and the scan's diagnostics in `d`; returns true when
+// the scan outgrew the group's scratch (rows or the row-key table).
+template <int W>
+__device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* seeds, int ns, double rho,
+                           int source_bins, unsigned long long epoch, unsigned long long& local_gen,
+                           double* areaimage, int* flags, Diag& d, double& area)
+{
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
+    const double nbin = static_cast<double>(max(source_bins, 1));
+    const double incr = rho / nbin;
+    C.max_steps = max(100000, source_bins * source_bins * 2000);
+    C.band = dmax_(4.0 * rho * incr, 4.0 * incr * incr);
+    C.step = incr;
+    C.tape_n = 0;
+    const double margin = 0.5 * incr * 1.01;
+    bool ovf = false;
+    for (int i = t; i < ns; i += N) {
+        areaimage[i] = 0.0;
+        flags[i] = 0;
+    }
+    Grp<W>::sync();
+    area = 0.0;
+    for (int ii = 0; ii < ns && !ovf; ++ii) {
+        if (flags[ii] & 1) continue;
+        ++local_gen;
+        R.gen = (epoch << 32) | (local_gen & 0xffffffffull);
+        R.hw = 0;
+        R.ovf = false;
+        rows_ensure<W>(R, 1);
+        const P2 seed = seeds[ii];
+        if (C.f32) C.A = make_anchor32(C.m, seed.x, seed.y, C.src);
+        double areai = 0.0;
+        double dy = incr;
+        int yi = 0;
+        const double jseed = jacobian(C.m, seed.x, seed.y);
+        const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
+        ++d.processed;
+        if (js != 0) ++d.fold;
+        wset<W>(R.xmin, 0, seed.x);
+        wset<W>(R.xmax, 0, seed.x);
+        Grp<W>::sync();
+        areai = image_area<W>(C, R, S, seed, dy, yi, js);
+        Grp<W>::sync();
+        dy = -incr;
+        rows_ensure<W>(R, yi);
+        if (R.ovf) {
+            ovf = true;
+            break;
+        }
+        const P2 lower{R.xmax[0], seed.y + dy};
+        {
+            const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
+            Grp<W>::sync();
+            wset<W>(R.xmin, yi, xm0);
+            wset<W>(R.xmax, yi, xM0);
+            wset<W>(R.y, yi, y0);
+            wset<W>(R.dys, yi, dy);
+            Grp<W>::sync();
+        }
+        ++yi;
+        areai += image_area<W>(C, R, S, lower, dy, yi, js);
+        Grp<W>::sync();
+        int nyi = yi;
+        double areabound = 0.0;
+        for (int row = 0; row < nyi && !R.ovf; ++row) {
+            rows_ensure<W>(R, row + 1);
+            const double dxmax = R.xmax[row + 1] - R.xmax[row];
+            const double dxmin = R.xmin[row + 1] - R.xmin[row];
+            if (R.ax[row + 1] > 0.0) d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
+            if (R.ax[row + 1] > 0.0) {
+                if (dxmax > 1.1 * incr) {
+                    ++d.gap_repairs;
+                    repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1],
+                              -R.dys[row], yi, js, areai, areabound);
+                }
+                if (dxmin > 1.1 * incr) {
+                    ++d.gap_repairs;
+                    repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row],
+                              R.xmin[row + 1], R.dys[row], yi, js, areai, areabound);
+                }
+                if (dxmin < -1.1 * incr) {
+                    ++d.gap_repairs;
+                    repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row],
+                              -R.dys[row], yi, js, areai, areabound);
+                }
+                if (dxmax < -1.1 * incr) {
+                    ++d.gap_repairs;
+                    repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1],
+                              R.xmax[row], R.dys[row], yi, js, areai, areabound);
+                }
+            }
+            if (row == nyi - 1 && areabound > 0.0 && yi > nyi) nyi = yi;
+        }
+        if (R.ovf) {
+            ovf = true;
+            break;
+        }
+        area += areai;
+        if (t == 0) areaimage[ii] = areai;
+        {
+            int br = 0;
+            for (int row = t; row < nyi; row += N) br += (R.ax[row] > 0.0) ? 1 : 0;
+            br = warp_sum_i(br);
+            if (W > 1) {
+                if (lane_id() == 0) S.red[warp_in_block()] = br;
+                __syncthreads();
+                br = 0;
+                for (int i = 0; i < W; ++i) br += S.red[i];
+                __syncthreads();
+            }
+            d.boundary_rows += br;
+        }
+        // Overlap bookkeeping against every other seed (FSM:2681-2739).
+        for (int oi = 0; oi < ns; ++oi) {
+            if (oi == ii) continue;
+            const P2 p = seeds[oi];
+            if (js != 0) {
+                if (sign_of(jacobian(C.m, p.x, p.y)) == -js) continue;
+                if (rho >= 4.0e-3 && source_bins >= 35 && oi > ii && fabs(jseed) < 1.0e-3 &&
+                    fabs(jacobian(C.m, p.x, p.y)) < 0.02)
+                    continue;
+            }
+            bool hit = false;
+            for (int r0 = 0; r0 < nyi; r0 += N) {
+                const int row = r0 + t;
+                bool h = false;
+                if (row < nyi && R.ax[row] > 0.0) {
+                    h = p.y >= R.y[row] - margin && p.y <= R.y[row] + margin &&
+                        p.x >= R.xmin[row] - margin && p.x <= R.xmax[row] + margin;
+                }
+                if (Grp<W>::any(h)) {
+                    hit = true;
+                    break;
+                }
+            }
+            if (hit) {
+                ++d.overlaps;
+                if (oi < ii) {
+                    const int f = flags[oi];
+                    if (!(f & 2)) {
+                        area -= areaimage[oi];
+                        Grp<W>::sync();
+                        if (t == 0) flags[oi] = f | 2;
+                    }
+                } else {
+                    if (t == 0) flags[oi] = flags[oi] | 1;
+                }
+                Grp<W>::sync();
+            }
+        }
+        Grp<W>::sync();
+    }
+    return ovf;
 }
 
 // The list a kernel instance works through.
@@ -785,185 +948,70 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
             C.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
             C.max_steps = max(100000, st.source_bins * st.source_bins * 2000);
             C.f32 = w.f32_rays != 0;
-            const double nbin = static_cast<double>(max(st.source_bins, 1));
-            const double incr = rho / nbin;
             // Adaptive local refinement records the scan's boundary cells, so
             // every cell goes through the reference's loop body (no bulk runs).
             const bool adaptive = tape && st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0);
             C.tape = adaptive ? tape : nullptr;
-            C.tape_n = 0;
             C.tape_max = max(64, st.max_source_bins);
             if (C.tape_max > kTapeMax) C.tape_max = kTapeMax;
-            C.band = dmax_(4.0 * rho * incr, 4.0 * incr * incr);
-            C.step = incr;
             if (adaptive) C.bulk = false;
-            const double margin = 0.5 * incr * 1.01;
-            Diag d{ns, 0, 0, 0, 0, 0, 0.0};
-            for (int i = t; i < ns; i += N) {
-                areaimage[i] = 0.0;
-                flags[i] = 0;
-            }
-            Grp<W>::sync();
-            double area = 0.0;
-            for (int ii = 0; ii < ns && !ovf; ++ii) {
-                if (flags[ii] & 1) continue;
-                ++local_gen;
-                R.gen = (epoch << 32) | (local_gen & 0xffffffffull);
-                R.hw = 0;
-                R.ovf = false;
-                rows_ensure<W>(R, 1);
-                const P2 seed = seeds[ii];
-                if (C.f32) C.A = make_anchor32(C.m, seed.x, seed.y, C.src);
-                double areai = 0.0;
-                double dy = incr;
-                int yi = 0;
-                const double jseed = jacobian(C.m, seed.x, seed.y);
-                const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
-                ++d.processed;
-                if (js != 0) ++d.fold;
-                wset<W>(R.xmin, 0, seed.x);
-                wset<W>(R.xmax, 0, seed.x);
-                Grp<W>::sync();
-                areai = image_area<W>(C, R, S, seed, dy, yi, js);
-                Grp<W>::sync();
-                dy = -incr;
-                rows_ensure<W>(R, yi);
-                if (R.ovf) {
-                    ovf = true;
-                    break;
+            // The scan, and the topology retry of fixed_inverse_ray_binary
+            // (FSM:3168-3196): when needs_global_topology_retry (FSM:1108-1121)
+            // holds, the same seeds are scanned again at
+            // min(max_source_bins, max(50, 2 source_bins)) bins, and that scan's
+            // magnification, diagnostics and tape replace the first one's
+            // (refinement level 1).  A retry that is not finite leaves the first
+            // scan's results, which a third scan at the original bins restores
+            // (its tape included).
+            const int retry_bins = min(st.max_source_bins, max(50, 2 * max(st.source_bins, 1)));
+            int bins = st.source_bins;  // the settings' source_bins of the current scan
+            int level0 = 0;
+            double err = 0.0, scale = 1.0;
+            for (int attempt = 0;; ++attempt) {
+                Diag d{ns, 0, 0, 0, 0, 0, 0.0};
+                double area = 0.0;
+                ovf = scan_point<W>(C, R, S, seeds, ns, rho, bins, epoch, local_gen, areaimage, flags, d, area);
+                if (ovf) break;
+                const double nb = static_cast<double>(max(bins, 1));
+                const double flux = source_flux(rho, st.ld_c, st.ld_d);
+                const double sc = flux / (rho * rho) * nb * nb;
+                const double a = area / sc;
+                if (attempt == 1 && !isfinite(a)) {
+                    bins = st.source_bins;
+                    continue;
                 }
-                const P2 lower{R.xmax[0], seed.y + dy};
-                {
-                    const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
-                    Grp<W>::sync();
-                    wset<W>(R.xmin, yi, xm0);
-                    wset<W>(R.xmax, yi, xM0);
-                    wset<W>(R.y, yi, y0);
-                    wset<W>(R.dys, yi, dy);
-                    Grp<W>::sync();
+                double e = area_error(d, rho, bins, st.ld_c, st.ld_d);
+                const double fc = floor_coefficient(d, a, rho);
+                if (fc > 0.0) e = dmax_(e, fabs(a) * (fc / nb));
+                A = a;
+                err = e;
+                scale = sc;
+                if (attempt == 1) level0 = 1;
+                if (attempt == 0 && isfinite(a) && st.adaptive_source_bins != 0 && st.source_bins < 50 &&
+                    st.max_source_bins > st.source_bins && rho < 1.0e-2 && d.seed_count >= 16 &&
+                    d.overlaps >= 100 && d.gap_repairs >= 1000 && d.max_jump >= 1000.0 &&
+                    retry_bins > st.source_bins) {
+                    bins = retry_bins;
+                    continue;
                 }
-                ++yi;
-                areai += image_area<W>(C, R, S, lower, dy, yi, js);
-                Grp<W>::sync();
-                int nyi = yi;
-                double areabound = 0.0;
-                for (int row = 0; row < nyi && !R.ovf; ++row) {
-                    rows_ensure<W>(R, row + 1);
-                    const double dxmax = R.xmax[row + 1] - R.xmax[row];
-                    const double dxmin = R.xmin[row + 1] - R.xmin[row];
-                    if (R.ax[row + 1] > 0.0) d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
-                    if (R.ax[row + 1] > 0.0) {
-                        if (dxmax > 1.1 * incr) {
-                            ++d.gap_repairs;
-                            repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1],
-                                      -R.dys[row], yi, js, areai, areabound);
-                        }
-                        if (dxmin > 1.1 * incr) {
-                            ++d.gap_repairs;
-                            repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row],
-                                      R.xmin[row + 1], R.dys[row], yi, js, areai, areabound);
-                        }
-                        if (dxmin < -1.1 * incr) {
-                            ++d.gap_repairs;
-                            repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row],
-                                      -R.dys[row], yi, js, areai, areabound);
-                        }
-                        if (dxmax < -1.1 * incr) {
-                            ++d.gap_repairs;
-                            repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1],
-                                      R.xmax[row], R.dys[row], yi, js, areai, areabound);
-                        }
-                    }
-                    if (row == nyi - 1 && areabound > 0.0 && yi > nyi) nyi = yi;
-                }
-                if (R.ovf) {
-                    ovf = true;
-                    break;
-                }
-                area += areai;
-                if (t == 0) areaimage[ii] = areai;
-                {
-                    int br = 0;
-                    for (int row = t; row < nyi; row += N) br += (R.ax[row] > 0.0) ? 1 : 0;
-                    br = warp_sum_i(br);
-                    if (W > 1) {
-                        if (lane_id() == 0) S.red[warp_in_block()] = br;
-                        __syncthreads();
-                        br = 0;
-                        for (int i = 0; i < W; ++i) br += S.red[i];
-                        __syncthreads();
-                    }
-                    d.boundary_rows += br;
-                }
-                // Overlap bookkeeping against every other seed (FSM:2681-2739).
-                for (int oi = 0; oi < ns; ++oi) {
-                    if (oi == ii) continue;
-                    const P2 p = seeds[oi];
-                    if (js != 0) {
-                        if (sign_of(jacobian(C.m, p.x, p.y)) == -js) continue;
-                        if (rho >= 4.0e-3 && st.source_bins >= 35 && oi > ii && fabs(jseed) < 1.0e-3 &&
-                            fabs(jacobian(C.m, p.x, p.y)) < 0.02)
-                            continue;
-                    }
-                    bool hit = false;
-                    for (int r0 = 0; r0 < nyi; r0 += N) {
-                        const int row = r0 + t;
-                        bool h = false;
-                        if (row < nyi && R.ax[row] > 0.0) {
-                            h = p.y >= R.y[row] - margin && p.y <= R.y[row] + margin &&
-                                p.x >= R.xmin[row] - margin && p.x <= R.xmax[row] + margin;
-                        }
-                        if (Grp<W>::any(h)) {
-                            hit = true;
-                            break;
-                        }
-                    }
-                    if (hit) {
-                        ++d.overlaps;
-                        if (oi < ii) {
-                            const int f = flags[oi];
-                            if (!(f & 2)) {
-                                area -= areaimage[oi];
-                                Grp<W>::sync();
-                                if (t == 0) flags[oi] = f | 2;
-                            }
-                        } else {
-                            if (t == 0) flags[oi] = flags[oi] | 1;
-                        }
-                        Grp<W>::sync();
-                    }
-                }
-                Grp<W>::sync();
+                break;
             }
             if (t == 0) w.rays[it] = C.rays;
             if (!ovf) {
-                const double flux = source_flux(rho, st.ld_c, st.ld_d);
-                const double scale = flux / (rho * rho) * nbin * nbin;
-                A = area / scale;
-                double err = area_error(d, rho, st.source_bins, st.ld_c, st.ld_d);
-                const double fc = floor_coefficient(d, A, rho);
-                if (fc > 0.0) err = dmax_(err, fabs(A) * (fc / static_cast<double>(max(st.source_bins, 1))));
                 o.err = isfinite(A) ? err : dnan();
                 const double target = st.tol + st.reltol * dmax_(fabs(A), 1.0);
                 o.converged = isfinite(A) && err <= 0.999 * target;
+                if (t == 0 && w.levels) w.levels[it] = level0;
                 if (C.tape && isfinite(A)) {
-                    // needs_global_topology_retry (FSM:1108-1121): the reference
-                    // would scan again at twice the bins; that rerun is not built.
-                    const bool retry = st.source_bins < 50 && st.max_source_bins > st.source_bins && rho < 1.0e-2 &&
-                                       d.seed_count >= 16 && d.overlaps >= 100 && d.gap_repairs >= 1000 &&
-                                       d.max_jump >= 1000.0 &&
-                                       min(st.max_source_bins, max(50, 2 * max(st.source_bins, 1))) > st.source_bins;
-                    Refined rf{A, err, 0, false};
-                    if (!retry && t == 0 && C.tape_n > 0) {
+                    const int active_bins = max(bins, 1);
+                    Refined rf{A, err, level0, false};
+                    if (t == 0 && C.tape_n > 0) {
                         // The row arrays are free once the scans are done: they hold the heap.
-                        rf = refine(C, st, A, err, scale, max(st.source_bins, 1), reinterpret_cast<RefCell*>(R.xmin),
+                        rf = refine(C, st, A, err, scale, active_bins, level0, reinterpret_cast<RefCell*>(R.xmin),
                                     static_cast<int>((5ll * cap * sizeof(double)) / sizeof(RefCell)));
                     }
-                    const int active_bins = max(st.source_bins, 1);
                     if (t == 0) {
-                        if (retry) {
-                            o.status = kFsTopologyRetry;
-                        } else if (rf.ovf) {
+                        if (rf.ovf) {
                             o.status = kFsRowOverflow;
                         } else {
                             A = rf.A;

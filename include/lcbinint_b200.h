@@ -343,16 +343,21 @@ int lcbi_gpu_last_refinement_levels(lcbi_gpu_context *ctx, int64_t n, int32_t *l
  * when the library's device code is loaded on that device:
  *   - settings->caustic_bins above LCBI_NOALLOC_MAX_CAUSTIC_BINS is rejected
  *     with LCBI_INVALID_ARGUMENT and a message in lcbi_gpu_last_error;
- *   - a point whose Cartesian scan needs more than 65536 rows, or whose polar
- *     flood fill holds more than 131072 segments, gets status 18 / 19 (the
- *     workspace entry points go on to 1048576).
- * The first call on a device does a one-time setup (it looks up the fixed
- * array's device address, which loads the library's device code on that device,
- * and uploads constant angle tables); make that first call -- n = 0 is enough --
- * before any stream capture begins.  Calls on one device share the one array:
- * calls that overlap in time (two host threads, or two streams without
- * ordering between them) race on it, so serialise them.  The call returns after
- * its work on the context's stream has finished. */
+ *   - adaptive local refinement (adaptive_source_bins with a tolerance) is
+ *     refused with LCBI_UNSUPPORTED: its tapes and heaps do not fit the array;
+ *   - a point whose Cartesian scan needs more than 65536 rows per seed, or
+ *     whose polar flood fill visits more than 262144 segments (or queues more
+ *     than 131072 at once), gets status 18 / 19 and NaN (the workspace entry
+ *     points go on to 524288 rows and 2097152 segments).
+ * The first call on a device sets up: it looks up the fixed array's device
+ * address (which loads the library's device code on that device) and uploads
+ * constant angle tables with a synchronous copy.  Make that first call -- n = 0
+ * is enough -- before any stream capture begins.  Every later call checks the
+ * set-up again and repeats it after a cudaDeviceReset.  Calls on one device
+ * share the one array and each leaves its contents behind (every call clears
+ * what must start empty): calls that overlap in time (two host threads, or two
+ * streams without ordering between them) race on it, so serialise them.  The
+ * call returns after its work on the context's stream has finished. */
 #define LCBI_NOALLOC_MAX_CAUSTIC_BINS 2048
 #define LCBI_NOALLOC_AREA_BYTES (48u << 20)
 int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, double s, double q,

@@ -13,7 +13,8 @@
 // kernel launches on the context's stream.
 //
 // Limits of the fixed area (LCBI_NOALLOC_* in the public header): caustic_bins
-// at most 2048 (larger requests are rejected); 2048 image seeds per point
+// at most 2048 (larger requests are rejected); adaptive local refinement
+// (adaptive_source_bins with a tolerance) is refused with LCBI_UNSUPPORTED; 2048 image seeds per point
 // (status 17 beyond, as in lcbi_gpu_binary_mag); 8192 rows per Cartesian seed
 // scan and 16384 polar segments in flight in the first pass (one warp per
 // point), with a second pass on four blocks (one point per block) at 65536
@@ -32,6 +33,8 @@
 #include "../../include/lcbinint_b200.h"
 #include "lcbi_context.h"
 #include "lcbi_fs_kernels.h"
+
+#include <cuda.h>
 
 #include <cmath>
 #include <complex>
@@ -97,6 +100,7 @@ namespace {
 struct DeviceArea {
     unsigned char* area;
     double2* trig;
+    unsigned long long context_id;  // the CUDA context the tables were uploaded in
     bool ready;
 };
 DeviceArea g_devices[kMaxDevices];
@@ -114,22 +118,55 @@ bool scratch_fits(size_t* main_cart, size_t* main_polar, size_t* retry_cart, siz
     return first <= kScratchBytes && second <= kScratchBytes;
 }
 
-// One-time setup for the context's device (the device must be current): looks
-// up the device addresses of the fixed arrays and uploads the angle tables,
-// evaluated with the host C library exactly like the workspace path does.
+// The unique id of the current CUDA context (cuCtxGetId, reached through the
+// runtime's driver entry points so that nothing links libcuda); 0 if unknown.
+// A cudaDeviceReset ends the device's primary context, and the next one gets
+// a new id.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || c == nullptr || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Set-up for the context's device (the device must be current), checked on
+// every call: looks up the device addresses of the fixed arrays (cheap once
+// the library's device code is loaded) and uploads the angle tables,
+// evaluated with the host C library exactly as the workspace path evaluates
+// them, whenever the device has not been set up in its current CUDA context:
+// on the device's first call, and again after a cudaDeviceReset, which loads
+// the device code afresh (the arrays may sit elsewhere and have lost their
+// contents).  The upload is a synchronous cudaMemcpy.
 bool setup(Context* ctx)
 {
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return ctx->fail("device index beyond the fixed-area table");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    DeviceArea& d = g_devices[ctx->device];
-    if (d.ready) return true;
-    size_t a, b, c, e;
-    if (!scratch_fits(&a, &b, &c, &e)) return ctx->fail("fixed-area scan sizes exceed the scratch part");
     void* area = nullptr;
     void* trig = nullptr;
     if (!ctx->check("cudaGetSymbolAddress(fixed area)", cudaGetSymbolAddress(&area, g_noalloc_area)) ||
         !ctx->check("cudaGetSymbolAddress(angle tables)", cudaGetSymbolAddress(&trig, g_noalloc_trig)))
         return false;
+    const unsigned long long cid = current_context_id();
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    DeviceArea& d = g_devices[ctx->device];
+    if (d.ready && d.area == area && d.trig == trig && d.context_id == cid) return true;
+    size_t a, b, c, e;
+    if (!scratch_fits(&a, &b, &c, &e)) return ctx->fail("fixed-area scan sizes exceed the scratch part");
     static double2 host[kTrig];
     int k = 0;
     const double phase_step = 2.0 * kHostPi / static_cast<double>(1400);
@@ -149,9 +186,11 @@ bool setup(Context* ctx)
         const double th = 2.0 * kHostPi * static_cast<double>(i) / static_cast<double>(16);
         host[k++] = make_double2(std::cos(th), std::sin(th));
     }
+    d.ready = false;
     if (!ctx->check("angle tables upload", cudaMemcpy(trig, host, sizeof(host), cudaMemcpyHostToDevice))) return false;
     d.area = static_cast<unsigned char*>(area);
     d.trig = static_cast<double2*>(trig);
+    d.context_id = cid;
     d.ready = true;
     return true;
 }
@@ -235,8 +274,13 @@ extern "C" int lcbi_gpu_binary_mag_noalloc(lcbi_gpu_context* c, const lcbi_fs_se
     if (!ctx->check("cudaSetDevice", cudaSetDevice(ctx->device)) || !setup(ctx)) return LCBI_GPU_ERROR;
     if (n == 0) return LCBI_OK;
     if (!y1 || !y2 || !rho || !results) return LCBI_INVALID_ARGUMENT;
-    unsigned char* area = g_devices[ctx->device].area;
-    const double2* trig = g_devices[ctx->device].trig;
+    unsigned char* area;
+    const double2* trig;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        area = g_devices[ctx->device].area;
+        trig = g_devices[ctx->device].trig;
+    }
     cudaStream_t st = ctx->stream;
 
     // Per-call constants: settings, the lens model with its phase table, the

@@ -17,8 +17,9 @@ GPU; e2e = the same through the host-pointer C ABI (host->device copies and
 result readback inside the timed region); roofline of the dominant kernel
 against the device-measured FP64 FMA peak; cpu_baseline = the reference
 compiled from source (oracle/_ref), one process per host core, on a bounded
-sample of the same points.  Under torchrun every rank runs its own batch
-(independent points: weak scaling, no data-path collective).
+sample of the same points.  Under torchrun the ranks' batches form one job
+split over the GPUs by estimated cost (independent points: weak scaling), and
+the only collective is the all-gather of the results.
 """
 from __future__ import annotations
 
@@ -920,7 +921,10 @@ def main():
     if args.workload != "fs_batch":
         run_other_workload(args, world, rank, local_rank, ncores)
         return
-    rows = fs_batch_workload(seed=1 + rank)
+    # One batch of 4,096 points per GPU; with several GPUs the batches form one
+    # job of 4,096 N points that is split over the ranks (weak scaling).
+    rows = np.concatenate([fs_batch_workload(seed=1 + r) for r in range(world)]) if world > 1 \
+        else fs_batch_workload(seed=1)
     if args.points > 0:
         rows = rows[np.random.default_rng(5).permutation(len(rows))[: args.points]]
     if args.point >= 0:
@@ -930,7 +934,10 @@ def main():
               "points": int(len(rows)), "models": 64,
               "precision": "fp64" if args.rays == "f64" else
                            "fp32 ray map about image-centred anchors, fp64 sums, fp64 seeds and decisions",
-              "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
+              "l2": "flushed between steps (256 MB write)",
+              "parallelism": "one GPU" if world == 1 else
+                             f"{world} GPUs: one batch of {len(rows)} points split by LPT on estimated cells "
+                             "(lcbinint_b200.shard), results all-gathered over NCCL inside the step"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -974,17 +981,34 @@ def main():
         ctx.check(L.lcbi_gpu_set_cell_budget(ctx.handle, 1), "lcbi_gpu_set_cell_budget")
         ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 2, 16384), "lcbi_gpu_set_workspace")
 
-    settings, models, pts = fs_batch_arrays(rows)
+    settings, models, pts_all = fs_batch_arrays(rows)
     st_arr = (LcbiStructs.FsSettings * len(settings))(*settings)
+    parts = None
+    if world > 1:
+        # Every rank computes the same partition from the same points.
+        from lcbinint_b200.shard import gather_results, lpt_partition, point_costs
+        a_ps = lb.binary_mag0_batch(pts_all["s"], pts_all["q"], pts_all["y1"], pts_all["y2"], device=local_rank)
+        parts = lpt_partition(point_costs(pts_all, settings, a_ps=a_ps), world)
+        pts = np.ascontiguousarray(pts_all[parts[rank]])
+        config["points_per_rank"] = [int(len(p)) for p in parts]
+    else:
+        pts = pts_all
     n = len(pts)
     d_pts = torch.from_numpy(pts.view(np.uint8).copy()).to(dev)
     d_res = torch.zeros(n * FS_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    if world > 1:
+        # The result gather: every rank's records, padded to the largest share.
+        g_in = torch.zeros(max(len(p) for p in parts) * FS_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        g_out = [torch.empty_like(g_in) for _ in range(world)]
 
     def step_device():
         rc = L.lcbi_gpu_binary_mag(ctx.handle, st_arr, len(settings), models.ctypes.data, len(models), n,
                                    d_pts.data_ptr(), d_res.data_ptr(), _lib.DEVICE_POINTERS | 2)
         ctx.check(rc, "lcbi_gpu_binary_mag")
+        if world > 1:
+            g_in[: d_res.numel()].copy_(d_res)
+            torch.distributed.all_gather(g_out, g_in)
 
     res_host = np.zeros(n, dtype=FS_RESULT_DTYPE)
 
@@ -992,6 +1016,8 @@ def main():
         rc = L.lcbi_gpu_binary_mag(ctx.handle, st_arr, len(settings), None, 0, n, pts.ctypes.data,
                                    res_host.ctypes.data, 0)
         ctx.check(rc, "lcbi_gpu_binary_mag")
+        if world > 1:
+            gather_results(res_host, parts, len(pts_all), device=dev)
 
     fp32_error = None
     if args.rays == "f32":

@@ -320,6 +320,18 @@ int lcbi_gpu_binary_geometry(lcbi_gpu_context *ctx, double s, double q, int32_t 
  * accounting; no reference counterpart.  n must not exceed that call's size. */
 int lcbi_gpu_last_ray_counts(lcbi_gpu_context *ctx, int64_t n, uint64_t *rays);
 
+/* Bounded device waits (no reference counterpart).  The tile-parallel flood
+ * fills (polar inverse ray, gradient lattice) hand tiles between persistent
+ * warps through a FIFO; a warp waiting for its ticket gives up after `polls`
+ * polls (0 restores the default, seconds of polling) and stops that flood.
+ * The polar flood's points are then integrated again by the
+ * one-block-per-point second pass, which does not wait on other warps, so
+ * magnifications never depend on whether a wait gave up (the gradients of a
+ * stopped gradient flood are NaN).  lcbi_gpu_last_wait_timeouts reports how
+ * many waits gave up during the last finite-source call on the context. */
+int lcbi_gpu_set_wait_limit(lcbi_gpu_context *ctx, uint32_t polls);
+int lcbi_gpu_last_wait_timeouts(lcbi_gpu_context *ctx, int32_t *count);
+
 /* FiniteSourceResult::refinement_level of each point of the last
  * finite-source call (finite_source_magnifier.hpp:58; 0 unless the point was
  * refined adaptively or scanned again at twice the bins).  n must not exceed

@@ -166,6 +166,10 @@ def _declare(L):
     L.lcbi_gpu_workspace_bytes.restype = C.c_int64
     L.lcbi_gpu_kernel_binary_version.argtypes = [_vp]
     L.lcbi_gpu_kernel_binary_version.restype = C.c_int
+    L.lcbi_gpu_set_wait_limit.argtypes = [_vp, C.c_uint32]
+    L.lcbi_gpu_set_wait_limit.restype = C.c_int
+    L.lcbi_gpu_last_wait_timeouts.argtypes = [_vp, _vp]
+    L.lcbi_gpu_last_wait_timeouts.restype = C.c_int
     L.lcbi_source_trajectory.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.lcbi_source_trajectory.restype = C.c_int
 

@@ -282,6 +282,8 @@ FsWork common_work(Context* ctx)
     w.seed_block_after = ctx->seed_block_after;
     w.seed_scratch = static_cast<char*>(ctx->fs_seed_block.ptr);
     w.seed_scratch_per_block = static_cast<long long>(seed_candidate_bytes_per_warp(ctx->cand_cap));
+    w.wait_limit = ctx->wait_limit;
+    w.wait_timeouts = static_cast<int*>(ctx->fs_waits.ptr);
     return w;
 }
 
@@ -532,6 +534,9 @@ bool prepare_tables(Context* ctx, const Plan& plan)
 // Per-point ray counts (and cycles) of n points, zeroed.
 bool prepare_counts(Context* ctx, long long n)
 {
+    if (!ctx->ensure(ctx->fs_waits, sizeof(int)) ||
+        !ctx->check("waits init", cudaMemsetAsync(ctx->fs_waits.ptr, 0, sizeof(int), ctx->stream)))
+        return false;
     if (!ctx->ensure(ctx->fs_levels, (size_t)(n + 1) * sizeof(int)) ||
         !ctx->check("levels init", cudaMemsetAsync(ctx->fs_levels.ptr, 0, (size_t)n * sizeof(int), ctx->stream)))
         return false;
@@ -1295,6 +1300,27 @@ int lcbi_gpu_last_ray_counts(lcbi_gpu_context* c, int64_t n, uint64_t* rays)
     if (ctx->fs_rays.ptr == nullptr || (size_t)n * sizeof(uint64_t) > ctx->fs_rays.bytes) return LCBI_INVALID_ARGUMENT;
     if (!ctx->check("rays D2H", cudaMemcpyAsync(rays, ctx->fs_rays.ptr, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                                                 ctx->stream)) ||
+        !ctx->finish())
+        return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_set_wait_limit(lcbi_gpu_context* c, uint32_t polls)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->wait_limit = polls;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_last_wait_timeouts(lcbi_gpu_context* c, int32_t* count)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !count) return LCBI_INVALID_ARGUMENT;
+    *count = 0;
+    if (ctx->fs_waits.ptr == nullptr) return LCBI_OK;
+    if (!ctx->check("waits D2H", cudaMemcpyAsync(count, ctx->fs_waits.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                                 ctx->stream)) ||
         !ctx->finish())
         return LCBI_GPU_ERROR;
     return LCBI_OK;

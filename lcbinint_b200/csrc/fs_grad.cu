@@ -276,6 +276,8 @@ struct GradCtx {
     unsigned* ring;
     GradCtl* ctl;
     unsigned long long mask;
+    unsigned spin_limit;      // polls before a wait gives up
+    int* timeouts;            // waits that gave up (null: not counted)
 };
 
 __device__ __forceinline__ unsigned long long gkey(int item, int ty, int tx)
@@ -697,8 +699,9 @@ __global__ void __launch_bounds__(128) grad_flood_kernel(GradCtx G)
                     stop = 1;
                     break;
                 }
-                if (spin >= kSpinLimit) {
+                if (spin >= G.spin_limit) {
                     atomicExch(&G.ctl->error, 1);
+                    if (G.timeouts) atomicAdd(G.timeouts, 1);
                     stop = 1;
                     break;
                 }
@@ -831,6 +834,8 @@ cudaError_t launch_grad(const FsWork& w, void* area, long long capacity, int max
     a = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(a) + 255) & ~uintptr_t(255));
     G.ctl = reinterpret_cast<GradCtl*>(a);
     G.mask = (unsigned long long)capacity - 1ull;
+    G.spin_limit = w.wait_limit ? w.wait_limit : kSpinLimit;
+    G.timeouts = w.wait_timeouts;
     cudaError_t e = cudaMemsetAsync(area, 0, (size_t)capacity * (sizeof(GradSlot) + sizeof(unsigned)), stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(G.ctl, 0, sizeof(GradCtl), stream);

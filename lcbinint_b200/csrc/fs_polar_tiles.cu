@@ -74,6 +74,8 @@ struct TileCtx {
     unsigned* ring;
     TileCtl* ctl;
     unsigned long long mask;  // capacity - 1 (table and ring)
+    unsigned spin_limit;      // polls before a wait gives up
+    int* timeouts;            // waits that gave up (null: not counted)
 };
 
 __device__ __forceinline__ unsigned long long tile_key(int item, int tphi, int tr)
@@ -329,8 +331,9 @@ __global__ void __launch_bounds__(128) tile_flood_kernel(TileCtx G)
                     stop = 1;
                     break;
                 }
-                if (spin >= kSpinLimit) {
+                if (spin >= G.spin_limit) {
                     atomicExch(&G.ctl->error, 1);
+                    if (G.timeouts) atomicAdd(G.timeouts, 1);
                     stop = 1;
                     break;
                 }
@@ -502,6 +505,8 @@ cudaError_t launch_polar_tiles(const FsWork& w, void* area, long long capacity, 
     a = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(a) + 255) & ~uintptr_t(255));
     G.ctl = reinterpret_cast<TileCtl*>(a);
     G.mask = (unsigned long long)capacity - 1ull;
+    G.spin_limit = w.wait_limit ? w.wait_limit : kSpinLimit;
+    G.timeouts = w.wait_timeouts;
     cudaError_t e = cudaMemsetAsync(area, 0, (size_t)capacity * (sizeof(TileSlot) + sizeof(unsigned)), stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(G.ctl, 0, sizeof(TileCtl), stream);

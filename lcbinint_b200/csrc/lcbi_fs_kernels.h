@@ -130,6 +130,13 @@ struct FsWork {
     const int* seed_count;
     int* seed_next;
     int seed_skip_early;
+    // Bounded device waits (the tile flood fills' FIFO tickets): a wait gives
+    // up after wait_limit polls (0: the default, seconds of polling), sets the
+    // flood's error word, and counts itself in *wait_timeouts (if not null);
+    // the points of a flood that gave up are integrated again by the second
+    // pass, which has no such waits.
+    unsigned wait_limit;
+    int* wait_timeouts;
 };
 
 constexpr int kEarlyMax = 32;

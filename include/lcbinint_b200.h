@@ -300,6 +300,16 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *se
                                const double *params, const int64_t *first, const int32_t *count,
                                const double *times, int64_t n_times, double *A, double *dA, int32_t *method,
                                int32_t *status);
+/* As lcbi_gpu_light_curves_grad, with the per-epoch arrays in device memory:
+ * times, A, dA (optional), method and status (optional) are DEVICE arrays of
+ * the context's device, so training loops keep them resident; params, first
+ * and count stay host arrays (they define the caustic models the host plans,
+ * 64 bytes per model).  No reference counterpart (the reference has no
+ * gradient). */
+int lcbi_gpu_light_curves_grad_device(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_models,
+                                      const double *params, const int64_t *first, const int32_t *count,
+                                      const double *times, int64_t n_times, double *A, double *dA,
+                                      int32_t *method, int32_t *status);
 
 /* Caustic (caustic != 0) or critical curve (caustic == 0) of a binary lens
  * (python/lcbinint_pybind.cpp:1882-1926, LightCurve.caustics /

@@ -170,6 +170,9 @@ def _declare(L):
     L.lcbi_gpu_set_wait_limit.restype = C.c_int
     L.lcbi_gpu_last_wait_timeouts.argtypes = [_vp, _vp]
     L.lcbi_gpu_last_wait_timeouts.restype = C.c_int
+    L.lcbi_gpu_light_curves_grad_device.argtypes = [_vp, _vp, C.c_int32, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp,
+                                                    _vp, _vp]
+    L.lcbi_gpu_light_curves_grad_device.restype = C.c_int
     L.lcbi_source_trajectory.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.lcbi_source_trajectory.restype = C.c_int
 

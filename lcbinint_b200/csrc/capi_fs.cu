@@ -900,11 +900,15 @@ int lcbi_gpu_light_curves(lcbi_gpu_context* c, const lcbi_fs_settings* settings,
     return LCBI_OK;
 }
 
-int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_models,
-                               const double* params, const int64_t* first, const int32_t* count, const double* times,
-                               int64_t n_times, double* A, double* dA, int32_t* method, int32_t* status)
+namespace {
+// lcbi_gpu_light_curves_grad with the per-epoch arrays (times, A, dA, method,
+// status) on the host (dev = false) or on the device (dev = true).  The
+// model parameters, first and count are host arrays either way: they define
+// the caustic models and the work the host plans.
+int light_curves_grad_impl(Context* ctx, const lcbi_fs_settings* settings, int32_t n_models, const double* params,
+                           const int64_t* first, const int32_t* count, const double* times, int64_t n_times,
+                           double* A, double* dA, int32_t* method, int32_t* status, bool dev)
 {
-    Context* ctx = reinterpret_cast<Context*>(c);
     if (!ctx || !settings || n_models < 0 || n_times < 0) return LCBI_INVALID_ARGUMENT;
     if (n_models == 0 || n_times == 0) return LCBI_OK;
     if (!params || !first || !count || !times || !A) return LCBI_INVALID_ARGUMENT;
@@ -950,15 +954,20 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* sett
         L.model = (p[6] != 0.0 && settings->finite_mode > 0) ? mt.get(L.s, L.q_core, settings->caustic_bins) : 0;
         L.pad = 0;
     }
-    if (!upload(ctx, ctx->fs_lc_models, lcm) || !ctx->ensure(ctx->fs_times, n_times * sizeof(double)) ||
-        !ctx->check("times H2D", cudaMemcpyAsync(ctx->fs_times.ptr, times, n_times * sizeof(double),
-                                                 cudaMemcpyHostToDevice, ctx->stream)) ||
-        !ctx->ensure(ctx->fs_items, n_times * sizeof(FsItem)) || !ctx->ensure(ctx->fs_out, n_times * sizeof(FsOut)) ||
+    const double* dt = times;
+    if (!upload(ctx, ctx->fs_lc_models, lcm) || !ctx->ensure(ctx->fs_items, n_times * sizeof(FsItem)) ||
+        !ctx->ensure(ctx->fs_out, n_times * sizeof(FsOut)) ||
         !ctx->ensure(ctx->fs_grad, (size_t)n_times * 8 * sizeof(double)) ||
         !ctx->ensure(ctx->fs_grad_lc, (size_t)n_times * 8 * sizeof(double)))
         return LCBI_GPU_ERROR;
+    if (!dev) {
+        if (!ctx->ensure(ctx->fs_times, n_times * sizeof(double)) ||
+            !ctx->check("times H2D", cudaMemcpyAsync(ctx->fs_times.ptr, times, n_times * sizeof(double),
+                                                     cudaMemcpyHostToDevice, ctx->stream)))
+            return LCBI_GPU_ERROR;
+        dt = static_cast<double*>(ctx->fs_times.ptr);
+    }
     const LcModel* dm = static_cast<LcModel*>(ctx->fs_lc_models.ptr);
-    const double* dt = static_cast<double*>(ctx->fs_times.ptr);
     if (!ctx->check("lc items", launch_lc_items(dm, n_models, dt, static_cast<FsItem*>(ctx->fs_items.ptr), n_times,
                                                 ctx->stream)))
         return LCBI_GPU_ERROR;
@@ -966,13 +975,22 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* sett
     double* pg = dA ? static_cast<double*>(ctx->fs_grad.ptr) : nullptr;
     if (!run_pipeline(ctx, plan, n_times, pg)) return LCBI_GPU_ERROR;
     if (dA) {
-        if (!ctx->check("gradient chain", launch_lc_grad_chain(dm, n_models, dt, pg,
-                                                               static_cast<double*>(ctx->fs_grad_lc.ptr), n_times,
-                                                               ctx->stream)) ||
-            !ctx->check("gradients D2H", cudaMemcpyAsync(dA, ctx->fs_grad_lc.ptr, (size_t)n_times * 8 * sizeof(double),
-                                                         cudaMemcpyDeviceToHost, ctx->stream)))
+        double* chain_out = dev ? dA : static_cast<double*>(ctx->fs_grad_lc.ptr);
+        if (!ctx->check("gradient chain", launch_lc_grad_chain(dm, n_models, dt, pg, chain_out, n_times, ctx->stream)))
             return LCBI_GPU_ERROR;
         ctx->launches += 1;
+        if (!dev && !ctx->check("gradients D2H", cudaMemcpyAsync(dA, ctx->fs_grad_lc.ptr,
+                                                                  (size_t)n_times * 8 * sizeof(double),
+                                                                  cudaMemcpyDeviceToHost, ctx->stream)))
+            return LCBI_GPU_ERROR;
+    }
+    if (dev) {
+        if (!ctx->check("results", launch_unpack_results(static_cast<const FsOut*>(ctx->fs_out.ptr), A, method, status,
+                                                         n_times, ctx->stream)) ||
+            !ctx->finish())
+            return LCBI_GPU_ERROR;
+        ctx->launches += 1;
+        return LCBI_OK;
     }
     std::vector<lcbi_fs_result> res(static_cast<size_t>(n_times));
     const int rc = finish_results(ctx, res.data(), n_times);
@@ -983,6 +1001,24 @@ int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* sett
         if (status) status[i] = res[i].status;
     }
     return LCBI_OK;
+}
+} // namespace
+
+int lcbi_gpu_light_curves_grad(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_models,
+                               const double* params, const int64_t* first, const int32_t* count, const double* times,
+                               int64_t n_times, double* A, double* dA, int32_t* method, int32_t* status)
+{
+    return light_curves_grad_impl(reinterpret_cast<Context*>(c), settings, n_models, params, first, count, times,
+                                  n_times, A, dA, method, status, false);
+}
+
+int lcbi_gpu_light_curves_grad_device(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int32_t n_models,
+                                      const double* params, const int64_t* first, const int32_t* count,
+                                      const double* times, int64_t n_times, double* A, double* dA, int32_t* method,
+                                      int32_t* status)
+{
+    return light_curves_grad_impl(reinterpret_cast<Context*>(c), settings, n_models, params, first, count, times,
+                                  n_times, A, dA, method, status, true);
 }
 
 } // extern "C"

@@ -125,4 +125,29 @@ cudaError_t launch_lc_grad_chain(const LcModel* models, int n_models, const doub
     return cudaGetLastError();
 }
 
+// Result records into separate device arrays (any of them may be null):
+// magnification, method and status of each point, as the host entry points
+// hand them back.
+__global__ void unpack_results_kernel(const FsOut* __restrict__ out, double* __restrict__ A, int* __restrict__ method,
+                                      int* __restrict__ status, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const FsOut o = out[i];
+        if (A) A[i] = o.A;
+        if (method) method[i] = o.method;
+        if (status) status[i] = o.status;
+    }
+}
+
+cudaError_t launch_unpack_results(const FsOut* out, double* A, int* method, int* status, long long n,
+                                  cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    unpack_results_kernel<<<(unsigned)blocks, 256, 0, stream>>>(out, A, method, status, n);
+    return cudaGetLastError();
+}
+
 } // namespace lcbi

@@ -219,6 +219,8 @@ cudaError_t launch_stash(const CausticModel* src_models, const P2* src_branches,
 cudaError_t launch_item_images(FsItem* items, long long n, double* a_ps, int* nimg, int sm_count, cudaStream_t stream);
 // Per-epoch gradients of light curves, (t0, tE, u0, alpha, s, q, rho, Gamma),
 // from the per-point gradients of launch_grad; `rho_sign` per model.
+cudaError_t launch_unpack_results(const FsOut* out, double* A, int* method, int* status, long long n,
+                                  cudaStream_t stream);
 cudaError_t launch_lc_grad_chain(const LcModel* models, int n_models, const double* times, const double* point_grads,
                                  double* grads, long long n_items, cudaStream_t stream);
 

@@ -197,3 +197,30 @@ def test_light_curve_autograd_matches_finite_differences():
     assert np.array_equal(At.detach().numpy(), A)
     At.sum().backward()
     assert np.allclose(params.grad.numpy(), dA.sum(axis=1), rtol=1e-12, atol=0)
+
+
+def test_device_resident_autograd_matches_the_host_arrays():
+    """Times, magnifications and gradients as CUDA tensors
+    (lcbi_gpu_light_curves_grad_device) give the host path's values bit for
+    bit, and torch.autograd runs through them on the device."""
+    import torch
+    from lcbinint_b200.autograd import light_curve_magnification, light_curves_with_grad
+    P = np.array([[0.0, 1.0, -0.01, 0.5, 0.95, 0.01, 5e-3, 0.5], [0.1, 20.0, 0.3, 0.7, 1.3, 0.01, 1e-3, 0.4],
+                  [-0.2, 15.0, 0.05, 2.0, 0.8, 0.05, 2e-3, 0.2]])
+    T = np.stack([np.linspace(-0.5, 0.5, 64), np.linspace(-30.0, 30.0, 64), np.linspace(-10.0, 10.0, 64)])
+    A, dA, method, status = light_curves_with_grad(P, T)
+    dev = torch.device("cuda", 0)
+    params = torch.tensor(P, device=dev, requires_grad=True)
+    times = torch.tensor(T, device=dev)
+    At = light_curve_magnification(params, times)
+    assert At.is_cuda
+    a = At.detach().cpu().numpy()
+    assert np.array_equal(np.isnan(a), np.isnan(A))
+    ok = ~np.isnan(A)
+    assert np.array_equal(a[ok].view(np.int64), A[ok].view(np.int64))
+    (At * torch.arange(64, device=dev, dtype=torch.float64)).sum().backward()
+    want = (dA * np.arange(64)[None, :, None]).sum(axis=1)
+    got = params.grad.cpu().numpy()
+    fin = np.isfinite(want)
+    assert np.array_equal(np.isfinite(got), fin)
+    assert np.allclose(got[fin], want[fin], rtol=1e-12, atol=0)

@@ -25,6 +25,7 @@
 #include "lcbi_fs_kernels.h"
 #include "lcbi_group.cuh"
 
+#include <atomic>
 #include <cstdint>
 
 namespace lcbi {
@@ -125,6 +126,7 @@ struct Ctx {
     double rho, rho2, inv_rho2;
     bool uniform;
     const double* ld;
+    const double* lds;        // the block's shared-memory copy of the same table (null: read ld)
     int max_steps;
     bool f32;                 // FP32 map about the current seed (A)
     Anchor32 A;
@@ -168,7 +170,8 @@ __device__ __forceinline__ void eval_for_scan(const Ctx& C, double x, double y, 
     const double d = ok ? md2 : C.rho2 + 1.0;
     *dz2 = d;
     double b = 0.0;
-    if (d <= C.rho2) b = C.uniform ? 1.0 : ld_lookup(C.ld, md2 * C.inv_rho2);
+    if (d <= C.rho2) b = C.uniform ? 1.0 : (C.lds ? ld_lookup_shared(C.lds, md2 * C.inv_rho2)
+                                                  : ld_lookup(C.ld, md2 * C.inv_rho2));
     *bright = b;
 }
 
@@ -236,21 +239,26 @@ __device__ __forceinline__ double advance(double x0, double d, int t)
     return x;
 }
 
-// Evaluates the chunk of cells starting at ix along dx into shared memory.
+// Evaluates the chunk of cells starting at ix along dx into shared memory:
+// cells [0, na).  With na < N the cells [na, N) hold a second segment, the
+// right scan (step -dx) of the row at sy from sx: the next row's first cells,
+// evaluated beside the current row's left scan (only left-scan fills carry
+// one).  na is a multiple of 32, so each warp evaluates one segment.
 template <int W>
 __device__ void fill_chunk(Ctx& C, CartShared<W>& S, double ix, double iy, double dx, int jsign, bool want_cont,
-                           double thr)
+                           double thr, int na, double sx, double sy)
 {
     const int t = Grp<W>::rank();
     Grp<W>::sync();  // every thread is done with the previous chunk
-    const double x = advance(ix, dx, t);
+    const bool first = t < na;
+    const double x = first ? advance(ix, dx, t) : advance(sx, -dx, t - na);
     double d, b;
-    eval_for_scan(C, x, iy, jsign, &d, &b);
+    eval_for_scan(C, x, first ? iy : sy, jsign, &d, &b);
     S.d[t] = d;
     S.b[t] = b;
     S.x[t] = x;
     const unsigned in = __ballot_sync(kFull, d <= C.rho2);
-    const unsigned co = __ballot_sync(kFull, want_cont && x >= thr);
+    const unsigned co = __ballot_sync(kFull, first && want_cont && x >= thr);
     if (lane_id() == 0) {
         S.in[t >> 5] = in;
         S.cont[t >> 5] = co;
@@ -259,20 +267,21 @@ __device__ void fill_chunk(Ctx& C, CartShared<W>& S, double ix, double iy, doubl
     Grp<W>::sync();
 }
 
-// First eventful chunk cell at or after `from`: an outside cell while
-// counting; otherwise an inside cell or one past the continue threshold.
+// First eventful chunk cell in [from, end): an outside cell while counting;
+// otherwise an inside cell or one past the continue threshold; end if none.
 template <int W>
-__device__ __forceinline__ int first_event(const CartShared<W>& S, int from, bool counting)
+__device__ __forceinline__ int first_event(const CartShared<W>& S, int from, int end, bool counting)
 {
     const int fw = from >> 5;
 #pragma unroll
     for (int w = 0; w < W; ++w) {
         if (w < fw) continue;
+        if ((w << 5) >= end) break;
         const unsigned lo = (w == fw) ? (kFull << (from & 31)) : kFull;
         const unsigned ev = counting ? (~S.in[w] & lo) : ((S.in[w] | ~S.cont[w]) & lo);
         if (ev) return (w << 5) + __ffs(ev) - 1;
     }
-    return Grp<W>::N;
+    return end;
 }
 
 // Sequential brightness sum of chunk cells [a, b) in order.  Every thread
@@ -282,7 +291,16 @@ __device__ __forceinline__ int first_event(const CartShared<W>& S, int from, boo
 template <int W>
 __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a, int b)
 {
-    for (int j = a; j < b; ++j) acc += S.b[j];
+    // Eight loads issued ahead of their additions, which stay in order.
+    int j = a;
+    for (; j + 8 <= b; j += 8) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = S.b[j + k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc += v[k];
+    }
+    for (; j < b; ++j) acc += S.b[j];
     return acc;
 }
 
@@ -320,23 +338,51 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
     int key = row_key(iy, inv_incr);
     unsigned pre_h = key_hash(key, R.tmask);
     ulonglong2 pre = R.table[pre_h];
-    // Chunk: cells [0, N) from (chunk start, cy) along cdx; cidx is the next one to consume.
+    // Chunk: cells [cidx, cend) from (chunk start, cy) along cdx; cidx is the
+    // next one to consume.  On a block, a left-scan fill of a row whose right
+    // scan has counted cells also evaluates the next row's first kSpecCells
+    // right-scan cells, in chunk cells [kSpecAt, N): that row starts at
+    // (cur_xmax - incr) + incr, one row up or down, and cur_xmax no longer
+    // changes once the row has a count.  The next row takes those cells when
+    // its start matches bit for bit (spec_x, spec_y), so every cell the scan
+    // consumes has the value a fill at that position would give.
+    constexpr bool kSpec = W > 1;
+    constexpr int kSpecCells = 32;
+    constexpr int kSpecAt = N - kSpecCells;
     bool have = false;
-    int cidx = 0;
+    int cidx = 0, cend = N;
     double cdx = 0.0, cy = 0.0;
+    bool spec = false;
+    double spec_x = 0.0, spec_y = 0.0;
     for (;;) {
-        if (!(have && cidx < N && cdx == dx && cy == iy)) {
-            if (C.budget > 0 && C.evals > C.budget) {
-                R.ovf = true;  // hand the point to the second pass
-                return countall;
+        if (!(have && cidx < cend && cdx == dx && cy == iy)) {
+            if (kSpec && spec && dx == incr && spec_x == ix && spec_y == iy) {
+                have = true;
+                cidx = kSpecAt;
+                cend = N;
+                cdx = dx;
+                cy = iy;
+                spec = false;
+            } else {
+                if (C.budget > 0 && C.evals > C.budget) {
+                    R.ovf = true;  // hand the point to the second pass
+                    return countall;
+                }
+                const bool want_cont = dx != incr && yi != 0;
+                const double thr = want_cont ? prev_xmin - dx : 0.0;
+                const bool next_row = kSpec && dx != incr && countx != 0.0;
+                const double nx = next_row ? (cur_xmax - incr) + incr : 0.0;
+                const double ny = next_row ? iy + dy : 0.0;
+                fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr, next_row ? kSpecAt : N, nx, ny);
+                have = true;
+                cidx = 0;
+                cend = next_row ? kSpecAt : N;
+                cdx = dx;
+                cy = iy;
+                spec = next_row;
+                spec_x = nx;
+                spec_y = ny;
             }
-            const bool want_cont = dx != incr && yi != 0;
-            const double thr = want_cont ? prev_xmin - dx : 0.0;
-            fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr);
-            have = true;
-            cidx = 0;
-            cdx = dx;
-            cy = iy;
         }
         // Bulk step: consume the run of cells that only accumulate (inside cells of
         // the right scan, or of the left scan once the row has a count) or only
@@ -347,7 +393,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
         if (C.bulk && guard + N + 2 < C.max_steps) {
             const bool counting = dx == incr || countx != 0.0;
             if (counting || yi != 0) {
-                const int stop = first_event<W>(S, cidx, counting);
+                const int stop = first_event<W>(S, cidx, cend, counting);
                 const int n = stop - cidx;
                 if (n > 0) {
                     if (counting) {
@@ -357,8 +403,8 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                     }
                     guard += n;
                     dz2 = S.d[stop - 1];
-                    if (stop == N) {
-                        ix = S.x[N - 1] + dx;
+                    if (stop == cend) {
+                        ix = S.x[cend - 1] + dx;
                         have = false;
                         continue;
                     }
@@ -885,8 +931,9 @@ struct CartList {
 
 template <int W>
 __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S,
-                               TapeCell* tape)
+                               TapeCell* tape, double* ld_smem = nullptr)
 {
+    int ld_loaded = -1;  // the limb-darkening table now in ld_smem
     constexpr int N = Grp<W>::N;
     const int t = Grp<W>::rank();
     const int cap = w.row_cap;
@@ -946,6 +993,18 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
             // I(r^2) >= 1 - c - d on [0, 1] for c, d >= 0, so every counted cell adds > 0.
             C.bulk = C.uniform || (st.ld_c >= 0.0 && st.ld_d >= 0.0 && st.ld_c + st.ld_d < 1.0);
             C.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
+            C.lds = nullptr;
+            if (ld_smem != nullptr && !C.uniform) {
+                // A block scan keeps its point's table in shared memory: the
+                // brightness lookup ends every cell's evaluation.
+                if (ld_loaded != st.ld_table) {
+                    Grp<W>::sync();
+                    for (int i = t; i <= kLdTable; i += Grp<W>::N) ld_smem[i] = C.ld[i];
+                    Grp<W>::sync();
+                    ld_loaded = st.ld_table;
+                }
+                C.lds = ld_smem;
+            }
             C.max_steps = max(100000, st.source_bins * st.source_bins * 2000);
             C.f32 = w.f32_rays != 0;
             // Adaptive local refinement records the scan's boundary cells, so
@@ -1050,13 +1109,17 @@ __global__ void __launch_bounds__(128, 2) cartesian_warp_kernel(FsWork w, unsign
                       w.tape ? w.tape + (long long)gw * kTapeMax : nullptr);
 }
 
+// Dynamic shared memory of the block kernel: one limb-darkening table.
+constexpr size_t kBlockLdBytes = (size_t)(kLdTable + 1) * sizeof(double);
+
 __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<kBigWarps> sh;
+    extern __shared__ double ld_smem[];
     const CartList L = w.early_pass ? CartList{w.early_cart, w.ir_count + 5, w.next_item + 6}
                                     : CartList{w.retry_cart, w.ir_count + 2, w.next_item + 3};
     cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
-                              w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr);
+                              w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr, ld_smem);
 }
 
 } // namespace
@@ -1073,7 +1136,20 @@ size_t cartesian_scratch_bytes(int row_cap, int seed_cap)
 cudaError_t launch_cartesian(const FsWork& w, int n_groups, cudaStream_t stream, unsigned long long epoch)
 {
     if (w.retry_pass) {
-        cartesian_block_kernel<<<n_groups, 32 * kBigWarps, 0, stream>>>(w, epoch);
+        // The shared-memory limit is a per-device attribute of the kernel, set
+        // before its first launch on each device (setting it again is harmless).
+        static std::atomic<unsigned long long> attr_set{0};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_set.load() & bit)) {
+            e = cudaFuncSetAttribute(cartesian_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kBlockLdBytes));
+            if (e != cudaSuccess) return e;
+            attr_set.fetch_or(bit);
+        }
+        cartesian_block_kernel<<<n_groups, 32 * kBigWarps, kBlockLdBytes, stream>>>(w, epoch);
     } else {
         cartesian_warp_kernel<<<(n_groups + 3) / 4, 128, 0, stream>>>(w, epoch);
     }

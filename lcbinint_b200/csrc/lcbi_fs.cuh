@@ -233,6 +233,14 @@ __device__ __forceinline__ double ld_lookup(const double* __restrict__ table, do
     return __ldg(table + static_cast<int>(r2 * static_cast<double>(kLdTable) + 0.5));
 }
 
+// The same lookup in a copy of the table held in shared memory.
+__device__ __forceinline__ double ld_lookup_shared(const double* table, double r2)
+{
+    if (r2 <= 0.0) return table[0];
+    if (r2 >= 1.0) return table[kLdTable];
+    return table[static_cast<int>(r2 * static_cast<double>(kLdTable) + 0.5)];
+}
+
 // ----- critical curve (FSM:528-567) -----
 
 // critical_curve_polynomial_coefficients with std::complex product semantics.

@@ -70,12 +70,21 @@ __device__ __forceinline__ double crit2(double ek)
     return t * t;
 }
 
-// Plain Laguerre iteration (cmplx_laguerre, SkowronGould.cpp:472-625), the
-// fallback when the three-regime solver does not converge in 80 steps.
+// A degree-N polynomial passed by value, so that a call that is not inlined
+// takes no address of the caller's coefficients (which then stay in registers).
 template <int N>
-__device__ __noinline__ void laguerre_fallback(const dc* poly, dc* root_io, bool* ok)
+struct PolyN {
+    dc c[N + 1];
+};
+
+// Plain Laguerre iteration (cmplx_laguerre, SkowronGould.cpp:472-625), the
+// fallback when the three-regime solver does not converge in 80 steps; returns
+// the root it reaches (its last iterate when it does not converge).  Rarely
+// taken, so kept out of line.
+template <int N>
+__device__ __noinline__ dc laguerre_fallback(const PolyN<N> pn, dc root)
 {
-    dc root = *root_io;
+    const dc* poly = pn.c;
     const double one_nth = 1.0 / N;
     const double n_1_nth = (N - 1.0) * one_nth;
     const double two_n_div_n_1 = 2.0 / n_1_nth;
@@ -86,10 +95,10 @@ __device__ __noinline__ void laguerre_fallback(const dc* poly, dc* root_io, bool
         double ek;
         horner<N, true>(poly, root, p, dp, d2, ek, true);
         const double abs2p = cnorm2(p);
-        if (abs2p == 0.0) { *root_io = root; return; }
+        if (abs2p == 0.0) return root;
         const double cr = crit2(ek);
         if (abs2p < cr) {
-            if (abs2p < 0.01 * cr) { *root_io = root; return; }
+            if (abs2p < 0.01 * cr) return root;
             good = true;
         } else {
             good = false;
@@ -108,13 +117,12 @@ __device__ __noinline__ void laguerre_fallback(const dc* poly, dc* root_io, bool
         if (czero(denom)) dx = cscale(absroot + 1.0, escape_dir(jump(i % 10) * 2 * 3.14159265358979323846));
         else dx = cdiv(fn, denom);
         dc nr = csub(root, dx);
-        if (ceq(nr, root)) { *root_io = root; return; }
-        if (good) { *root_io = nr; return; }
+        if (ceq(nr, root)) return root;
+        if (good) return nr;
         if (i % 10 == 0) nr = csub(root, cscale(jump((i / 10 - 1) % 10), dx));
         root = nr;
     }
-    *ok = false;
-    *root_io = root;
+    return root;
 }
 
 // Three-regime solver (cmplx_laguerre2newton, SkowronGould.cpp:764-1130),
@@ -293,9 +301,10 @@ __device__ __forceinline__ dc deflate_step(dc* p2)
 {
     dc root{0.0, 0.0};
     if (!laguerre2newton<N>(p2, root)) {
-        root = dc{0.0, 0.0};
-        bool ok = true;
-        laguerre_fallback<N>(p2, &root, &ok);
+        PolyN<N> pn;
+#pragma unroll
+        for (int i = 0; i <= N; ++i) pn.c[i] = p2[i];
+        root = laguerre_fallback<N>(pn, dc{0.0, 0.0});
     }
     dc coef = p2[N];
 #pragma unroll

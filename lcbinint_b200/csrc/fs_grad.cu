@@ -31,7 +31,9 @@
 //   continuum magnification (slot 6 of the output), O(h^2) from it, with no
 //   division by the lens map's point gradient, which vanishes where a contour
 //   meets a critical curve.
-//   Quadratic limb darkening (d != 0) is not differentiated (NaN).
+//   Quadratic limb darkening, I = 1 - c (1 - mu) - d (1 - sqrt(mu)), adds
+//   d int_0^1 U(rho sqrt(1 - u^4)) du, six more radii on a second contour
+//   pass that points without a quadratic term skip.
 #include "lcbi_fs_kernels.h"
 #include "lcbi_ps.cuh"
 #include "lcbi_warp.cuh"
@@ -43,7 +45,9 @@ namespace lcbi {
 namespace {
 
 constexpr double kSqrtHalf = 0.70710678118654752440;
-constexpr int kRadii = 7;       // rho and 6 Gauss-Legendre nodes of phi in [0, pi/2]
+constexpr int kRadiiLin = 7;    // rho and 6 Gauss-Legendre nodes of phi in [0, pi/2]
+constexpr int kRadiiQuad = 6;   // 6 Gauss-Legendre nodes of u in [0, 1]: the quadratic term
+constexpr int kRadii = kRadiiLin + kRadiiQuad;
 constexpr int kAcc = 6;         // U, dU/dy1, dU/dy2, dU/ds, dU/dq, dU/dR per radius
 constexpr int kKeyBits = 25;
 constexpr unsigned long long kKeyMask = (1ull << kKeyBits) - 1;
@@ -256,7 +260,7 @@ enum : int { kGActive = 0, kGDone = 1, kGOverflow = 2 };
 struct GradItem {
     LensDeriv L;
     P2 src;
-    double rho, c, h, tau;
+    double rho, c, d, h, tau;
     double R[kRadii];
     double acc[kRadii][kAcc];
     int state;
@@ -586,6 +590,7 @@ __global__ void __launch_bounds__(128) grad_phantom_kernel(GradCtx G)
 // derivatives exact for the linear interpolant).  Warp per tile (the tile of
 // the squares' lower-left cells); lane j owns row j and takes row j + 1 from
 // lane j + 1 (lane 31 evaluates row 32).
+template <int K0, int NK>
 __global__ void __launch_bounds__(128) grad_contour_kernel(GradCtx G)
 {
     const int j = lane_id();
@@ -600,6 +605,7 @@ __global__ void __launch_bounds__(128) grad_contour_kernel(GradCtx G)
         const int ty = static_cast<int>((k1 >> kKeyBits) & kKeyMask) - kKeyOffset;
         const int tx = static_cast<int>(k1 & kKeyMask) - kKeyOffset;
         if (G.items[item].state != kGActive) continue;
+        if (K0 >= kRadiiLin && G.items[item].d == 0.0) continue;  // no quadratic term
         // Visited bits of the tile's cells and of the cells just right of and
         // above it (neighbouring tiles), as 33-bit rows.
         long long sr = -1, su = -1, sru = -1;
@@ -628,11 +634,11 @@ __global__ void __launch_bounds__(128) grad_contour_kernel(GradCtx G)
         I.c = Ig.c;
         I.h = Ig.h;
         I.tau = Ig.tau;
-        double R[kRadii];
-        for (int k = 0; k < kRadii; ++k) R[k] = Ig.R[k];
-        double acc[kRadii][kAcc];
+        double R[NK];
+        for (int k = 0; k < NK; ++k) R[k] = Ig.R[K0 + k];
+        double acc[NK][kAcc];
 #pragma unroll
-        for (int k = 0; k < kRadii; ++k)
+        for (int k = 0; k < NK; ++k)
 #pragma unroll
             for (int a = 0; a < kAcc; ++a) acc[k][a] = 0.0;
         const int iy = ty * 32 + j;
@@ -657,7 +663,7 @@ __global__ void __launch_bounds__(128) grad_contour_kernel(GradCtx G)
             if (j == 31) c11 = own32;
             if (V & (1u << c)) {
 #pragma unroll
-                for (int k = 0; k < kRadii; ++k) {
+                for (int k = 0; k < NK; ++k) {
                     double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                     triangle(c00, c10, c11, false, R[k], I.h, t);
                     triangle(c00, c11, c01, true, R[k], I.h, t);
@@ -669,13 +675,13 @@ __global__ void __launch_bounds__(128) grad_contour_kernel(GradCtx G)
             c01 = c11;
         }
 #pragma unroll
-        for (int k = 0; k < kRadii; ++k) {
+        for (int k = 0; k < NK; ++k) {
 #pragma unroll
             for (int a = 0; a < kAcc; ++a) {
                 double v = acc[k][a];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-                if (j == ((k * kAcc + a) & 31) && v != 0.0) atomicAdd(&G.items[item].acc[k][a], v);
+                if (j == ((k * kAcc + a) & 31) && v != 0.0) atomicAdd(&G.items[item].acc[K0 + k][a], v);
             }
         }
     }
@@ -738,11 +744,16 @@ __global__ void __launch_bounds__(128) grad_start_kernel(FsWork w, GradCtx G, in
         I.src = P2{item.x, item.y};
         I.rho = item.rho;
         I.c = st.ld_c;
+        I.d = st.ld_d;
         I.h = item.rho / static_cast<double>(grad_bins);
         I.tau = 2.0 * I.h;
         I.R[0] = item.rho;
         for (int q = 0; q < 6; ++q) I.R[1 + q] = item.rho * sin(0.25 * kPi * (kGLx[q] + 1.0));
-        I.state = (st.ld_d == 0.0 && item.rho > 0.0) ? kGActive : kGDone;
+        for (int q = 0; q < 6; ++q) {
+            const double u = 0.5 * (kGLx[q] + 1.0);
+            I.R[kRadiiLin + q] = item.rho * sqrt(1.0 - u * u * u * u);
+        }
+        I.state = item.rho > 0.0 ? kGActive : kGDone;
     }
     if (lane_id() == 0) G.items[k] = I;
     __syncwarp();
@@ -773,10 +784,16 @@ __global__ void grad_finish_kernel(FsWork w, GradCtx G, double* grads)
     const FsOut o = w.out[I.slot_item];
     double res[8] = {dnan(), dnan(), dnan(), dnan(), dnan(), dnan(), o.A, static_cast<double>(o.method)};
     if (I.state == kGActive && G.ctl->error == 0) {
-        const double c = I.c;
-        double N = (1.0 - c) * I.acc[0][0];
-        double dN[4], dNR = (1.0 - c) * I.acc[0][5], dNc = -I.acc[0][0];
-        for (int a = 0; a < 4; ++a) dN[a] = (1.0 - c) * I.acc[0][1 + a];
+        // Layer-cake form of the brightness integral: with I(t) the law at
+        // t = r / rho, int_D I = I(1) U(rho) + int_0^1 (-I'(t)) U(rho t) dt.
+        // The linear term, c t / sqrt(1 - t^2), takes t = sin(phi); the
+        // quadratic one, (d t / 2)(1 - t^2)^(-3/4), takes u = (1 - t^2)^(1/4),
+        // which makes it d int_0^1 U(rho sqrt(1 - u^4)) du.
+        const double c = I.c, d = I.d;
+        const double edge = 1.0 - c - d;
+        double N = edge * I.acc[0][0];
+        double dN[4], dNR = edge * I.acc[0][5], dNc = -I.acc[0][0];
+        for (int a = 0; a < 4; ++a) dN[a] = edge * I.acc[0][1 + a];
         for (int q = 0; q < 6; ++q) {
             const double phi = 0.25 * kPi * (kGLx[q] + 1.0);
             const double wq = 0.25 * kPi * kGLw[q];
@@ -786,7 +803,18 @@ __global__ void grad_finish_kernel(FsWork w, GradCtx G, double* grads)
             for (int a = 0; a < 4; ++a) dN[a] += c * wq * I.acc[1 + q][1 + a] * sp;
             dNR += c * wq * I.acc[1 + q][5] * sp * sp;
         }
-        const double Phi = kPi * I.rho * I.rho * (1.0 - c / 3.0);
+        if (d != 0.0) {
+            for (int q = 0; q < 6; ++q) {
+                const double u = 0.5 * (kGLx[q] + 1.0);
+                const double vq = 0.5 * kGLw[q];
+                const double f = sqrt(1.0 - u * u * u * u);  // dR / drho
+                const double* acc = I.acc[kRadiiLin + q];
+                N += d * vq * acc[0];
+                for (int a = 0; a < 4; ++a) dN[a] += d * vq * acc[1 + a];
+                dNR += d * vq * acc[5] * f;
+            }
+        }
+        const double Phi = kPi * I.rho * I.rho * (1.0 - c / 3.0 - d / 5.0);
         const double A = N / Phi;
         for (int a = 0; a < 4; ++a) res[a] = dN[a] / Phi;
         res[4] = dNR / Phi - 2.0 * A / I.rho;
@@ -843,7 +871,8 @@ cudaError_t launch_grad(const FsWork& w, void* area, long long capacity, int max
     grad_start_kernel<<<(max_items * 32 + 127) / 128, 128, 0, stream>>>(w, G, grad_bins);
     grad_flood_kernel<<<flood_blocks, 128, 0, stream>>>(G);
     grad_phantom_kernel<<<sm_count * 8, 128, 0, stream>>>(G);
-    grad_contour_kernel<<<sm_count * 8, 128, 0, stream>>>(G);
+    grad_contour_kernel<0, kRadiiLin><<<sm_count * 8, 128, 0, stream>>>(G);
+    grad_contour_kernel<kRadiiLin, kRadiiQuad><<<sm_count * 8, 128, 0, stream>>>(G);
     grad_finish_kernel<<<(max_items + 127) / 128, 128, 0, stream>>>(w, G, grads);
     return cudaGetLastError();
 }

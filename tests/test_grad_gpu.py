@@ -224,3 +224,32 @@ def test_device_resident_autograd_matches_the_host_arrays():
     fin = np.isfinite(want)
     assert np.array_equal(np.isfinite(got), fin)
     assert np.allclose(got[fin], want[fin], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_quadratic_limb_darkening_gradient_matches_its_continuum_value(mode):
+    """Quadratic limb darkening (d != 0): finite gradients whose continuum value
+    agrees with the lattice forward, and which match finite differences of that
+    value in the source position, s, q and rho, at the linear law's bars."""
+    import lcbinint_b200 as lb
+    rows = _near_caustic(16, seed=13 + mode, rho_range=(3e-3, 1e-2), spread=1.0)
+    st = lb.Options(nbin=50).fs_settings(lb.LimbDarkening.quadratic(0.3, 0.25))
+    st.finite_mode = mode
+    st.kinji_threshold = 1e18
+    st.hex_threshold = 0.0
+    st.adaptive_hex_threshold = 0.0
+    sidx = np.zeros(len(rows))
+    res, g = _run(np.column_stack([rows, sidx]), [st])
+    assert (res["method"] == mode + 1).all() and (res["status"] == 0).all()
+    assert np.all(np.isfinite(g[:, :7]))
+    A = res["magnification"]
+    Ac = g[:, 6]
+    assert np.max(np.abs(Ac / A - 1.0)) < 2e-2, np.max(np.abs(Ac / A - 1.0))
+    rho = rows[:, 4]
+    for k, h, size in ((0, 1e-4 * rho, rho), (1, 1e-4 * rho, rho), (2, 1e-6 * rows[:, 0], rows[:, 0]),
+                       (3, 1e-6 * rows[:, 1], rows[:, 1]), (4, 1e-4 * rho, rho)):
+        _, _, gu, gd = _fd(rows, sidx, [st], k, h)
+        fd = (gu[:, 6] - gd[:, 6]) / (2 * h)
+        err = np.abs(g[:, k] - fd) * size / Ac
+        assert np.median(err) < 2e-3 and np.percentile(err, 75) < 1e-2, \
+            (k, np.median(err), np.percentile(err, 75), np.max(err))

@@ -284,8 +284,8 @@ int lcbi_gpu_light_curves(lcbi_gpu_context *ctx, const lcbi_fs_settings *setting
  * magnification the lattice approximates -- image-boundary contour integrals
  * at rho and six Gauss-Legendre radii, which carry the limb-darkening term
  * without its interior singularity, on a lattice of rho/48 cells (slot 6 holds
- * the continuum value).  Quadratic limb darkening (d != 0) gives NaN for
- * inverse-ray points. */
+ * the continuum value); quadratic limb darkening (d != 0) adds six radii
+ * rho sqrt(1 - u^4) at Gauss-Legendre nodes u of [0, 1]. */
 int lcbi_gpu_binary_mag_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_settings,
                              const lcbi_lens_model *models, int32_t n_models, int64_t n,
                              const lcbi_fs_point *points, lcbi_fs_result *results, double *grads,

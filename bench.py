@@ -659,6 +659,40 @@ def run_other_workload(args, world, rank, local_rank, ncores):
         print(json.dumps(out))
 
 
+def adjoint_forward_error(P, T, A, method, device, n_sample=96, seed=17):
+    """Relative error of the adjoint workload's forward magnifications against
+    a converged finite-source value on a random sample of its finite-source
+    epochs (hexadecapole and inverse ray): the same source forced to Cartesian
+    inverse ray at nbin 400, whose own convergence is shown by nbin 800."""
+    import lcbinint_b200 as lb
+    M, K = T.shape
+    fs = np.nonzero(method.ravel() >= 1)[0]
+    if fs.size == 0:
+        return None
+    idx = np.random.default_rng(seed).choice(fs, min(n_sample, fs.size), replace=False)
+    m, e = np.divmod(idx, K)
+    t0, tE, u0, al, s_, q_, rho, gam = (P[m, j] for j in range(8))
+    tau = (T[m, e] - t0) * (1.0 / tE)
+    y1 = tau * np.cos(al) - u0 * np.sin(al)
+    y2 = tau * np.sin(al) + u0 * np.cos(al)
+    conv = {}
+    for nb in (400, 800):
+        vals = np.empty(idx.size)
+        for g in np.unique(gam[:]):
+            sel = gam == g
+            vals[sel] = lb.binary_inverse_ray_batch(s_[sel], 1.0 / q_[sel], y1[sel], y2[sel], np.abs(rho[sel]),
+                                                    lb.LimbDarkening.linear(float(g)),
+                                                    lb.Options(inverse_ray_grid="cartesian", nbin=nb), device=device)
+        conv[nb] = vals
+    err = np.abs(A.ravel()[idx] / conv[800] - 1.0)
+    ref = np.abs(conv[400] / conv[800] - 1.0)
+    return {"vs": "forced Cartesian inverse ray at nbin 800 on the same epochs", "points": int(idx.size),
+            "median_rel": float(np.median(err)), "p90_rel": float(np.quantile(err, 0.9)),
+            "max_rel": float(err.max()), "frac_within_1e-4": float(np.mean(err <= 1e-4)),
+            "reference_convergence": {"nbin 400 vs 800 median_rel": float(np.median(ref)),
+                                      "max_rel": float(ref.max())}}
+
+
 def run_adjoint(args, world, rank, local_rank, ncores, common):
     """Adjoint workload: magnifications and their gradients in (t0, tE, u0, alpha, s,
     q, rho, Gamma) for 256 models x 500 epochs through the library's adjoint
@@ -750,6 +784,7 @@ def run_adjoint(args, world, rank, local_rank, ncores, common):
                e2e={"value": value, "unit": "magnifications/s", "h2d_bytes_per_step": int(P.nbytes + T.nbytes),
                     "d2h_bytes_per_step": int(n * 8 * 9)},
                gpu_launches=int(launches), clocks=clocks.summary())
+    out["forward_error"] = adjoint_forward_error(P, T, A, method, local_rank)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         rate, nn, wall = cpu_adjoint_rate(P, T, ncores, max(ncores, 32))
         out["cpu_baseline"] = {"value": rate, "unit": "magnifications/s", "cores": ncores, "kind": "reference",

@@ -465,6 +465,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
             if (pre_h == last_slot) pre = last_entry;
             unsigned slot;
             int e;
+            bool probed = false;
             if (pre.x != R.gen) {
                 slot = pre_h;
                 e = -1;
@@ -473,6 +474,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 e = (int)(pre.y & 0xffffffffull) - 1;
             } else {
                 e = key_lookup(R, key, &slot);
+                probed = true;
                 if (slot == 0xffffffffu) {
                     R.ovf = true;
                     return countall;
@@ -483,6 +485,13 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 if (cur_xmin + incr < R.xmax[e] && cur_xmax - incr > R.xmin[e]) return countall - countx;
                 e = R.next[e];
             }
+            // A probe read the table now, and rank 0 is about to write this
+            // row's entry into it: every thread of the group must have read
+            // the table first, or one that lags would find the row's own
+            // entry and take the row for an overlap with itself.  (The
+            // prefetched slot of the fast paths was read before any write of
+            // this row.)
+            if (probed) Grp<W>::sync();
             last_slot = slot;
             last_entry = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
                                                     (unsigned long long)(unsigned)(yi + 1));

@@ -331,10 +331,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
     rows_ensure<W>(R, yi);
     if (R.ovf) return countall;
     if (yi > 0) prev_xmin = R.xmin[yi - 1];
-    // Row-key table slot of the current row, fetched ahead; the slot rank 0
-    // wrote last is patched in, since the fetch may predate that write.
-    unsigned long long last_slot = ~0ull;
-    ulonglong2 last_entry = make_ulonglong2(0ull, 0ull);
+    // Row-key table slot of the current row, fetched ahead.
     int key = row_key(iy, inv_incr);
     unsigned pre_h = key_hash(key, R.tmask);
     ulonglong2 pre = R.table[pre_h];
@@ -462,10 +459,8 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 break;
             }
             // Same-row overlap with an earlier row of this seed's scans (FSM:1990-1999).
-            if (pre_h == last_slot) pre = last_entry;
             unsigned slot;
             int e;
-            bool probed = false;
             if (pre.x != R.gen) {
                 slot = pre_h;
                 e = -1;
@@ -474,7 +469,6 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 e = (int)(pre.y & 0xffffffffull) - 1;
             } else {
                 e = key_lookup(R, key, &slot);
-                probed = true;
                 if (slot == 0xffffffffu) {
                     R.ovf = true;
                     return countall;
@@ -485,20 +479,18 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 if (cur_xmin + incr < R.xmax[e] && cur_xmax - incr > R.xmin[e]) return countall - countx;
                 e = R.next[e];
             }
-            // A probe read the table now, and rank 0 is about to write this
-            // row's entry into it: every thread of the group must have read
-            // the table first, or one that lags would find the row's own
-            // entry and take the row for an overlap with itself.  (The
-            // prefetched slot of the fast paths was read before any write of
-            // this row.)
-            if (probed) Grp<W>::sync();
-            last_slot = slot;
-            last_entry = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
-                                                    (unsigned long long)(unsigned)(yi + 1));
-            if (Grp<W>::rank() == 0) {
-                R.next[yi] = head;
-                R.table[slot] = last_entry;
-            }
+            // The row's entry goes into the table.  Every thread of the group
+            // must have finished this row's reads of the table first (a row
+            // can end inside the cells evaluated ahead, with no other group
+            // barrier in it): a thread that lagged would otherwise find the
+            // row's own entry and take the row for an overlap with itself.
+            // Every thread then stores the same entry, so each one's later
+            // probes see all rows up to this one in its own program order
+            // and stop on the same slots as every other thread's.
+            Grp<W>::sync();
+            R.table[slot] = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
+                                                       (unsigned long long)(unsigned)(yi + 1));
+            if (Grp<W>::rank() == 0) R.next[yi] = head;
             ++yi;
             rows_ensure<W>(R, yi);
             if (R.ovf) return countall;

@@ -123,6 +123,8 @@ class _FsLib(_Lib):
         st = C.POINTER(FsSettings)
         f("binary_mag").argtypes = [st] + [C.c_double] * 6 + [C.c_int, _dp, _ip]
         f("inverse_ray_many").argtypes = [st, C.c_int] + [_dp] * 6 + [_ip]
+        if prefix == "orc_":
+            f("inverse_ray_many_fixed").argtypes = [st, C.c_int] + [_dp] * 6 + [_ip, _dp, C.c_void_p]
         f("seeds").argtypes = [st] + [C.c_double] * 5 + [_dp, C.c_int]
         f("cartesian").argtypes = [st] + [C.c_double] * 5 + [_dp, C.c_int, _dp]
         f("cartesian").restype = C.c_double
@@ -151,6 +153,20 @@ class _FsLib(_Lib):
         self.fn("inverse_ray_many")(C.byref(st), n, _ptr(s), _ptr(q), _ptr(x), _ptr(y), _ptr(rho),
                                     _ptr(A), _ptr(m, _ip))
         return A, m
+
+    def inverse_ray_fixed(self, st, s, q, x, y, rho):
+        """inverse_ray plus, for polar points, the integral with its cells summed
+        exactly the device's way (a 128-bit fixed-point sum) and the cell count."""
+        s, q, x, y, rho = (_f64(np.broadcast_to(v, np.broadcast(s, q, x, y, rho).shape)).ravel()
+                           for v in (s, q, x, y, rho))
+        n = s.size
+        A = np.empty(n)
+        m = np.empty(n, dtype=np.int32)
+        Af = np.empty(n)
+        cells = np.zeros(n, dtype=np.uint64)
+        self.fn("inverse_ray_many_fixed")(C.byref(st), n, _ptr(s), _ptr(q), _ptr(x), _ptr(y), _ptr(rho),
+                                          _ptr(A), _ptr(m, _ip), _ptr(Af), cells.ctypes.data)
+        return A, m, Af, cells
 
     def seeds(self, st, s, q, x, y, rho, cap=512):
         out = np.zeros(2 * cap)

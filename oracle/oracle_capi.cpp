@@ -118,6 +118,25 @@ void orc_inverse_ray_many(const CSettings* cst, int n, const double* s, const do
     }
 }
 
+// orc_inverse_ray_many, and for each polar point also its integral with the
+// cells summed exactly as the device sums them (NaN for other methods) and
+// the number of cells counted.
+void orc_inverse_ray_many_fixed(const CSettings* cst, int n, const double* s, const double* q, const double* x,
+                                const double* y, const double* rho, double* A, int* method, double* A_fixed,
+                                unsigned long long* cells)
+{
+    oracle::PolarFixedSum fx;
+    for (int i = 0; i < n; ++i) {
+        fx.value = std::nan("");
+        fx.cells = 0;
+        oracle::g_polar_fixed = &fx;
+        orc_inverse_ray_many(cst, 1, s + i, q + i, x + i, y + i, rho + i, A + i, method ? method + i : nullptr);
+        oracle::g_polar_fixed = nullptr;
+        A_fixed[i] = fx.value;
+        cells[i] = fx.cells;
+    }
+}
+
 int orc_seeds(const CSettings* st, double s, double q, double x, double y, double rho, double* out, int cap)
 {
     const auto v = oracle::seeds(conv(st), s, q, x, y, rho);

@@ -13,6 +13,9 @@
 #include <vector>
 
 namespace oracle {
+
+thread_local PolarFixedSum* g_polar_fixed = nullptr;
+
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
@@ -965,6 +968,30 @@ double cartesian_impl(const FsSettings& st, const LdTable& ld, double s, double 
 
 // ----- polar flood fill (FSM:1123-1364) -----
 
+// When set, polar_impl also sums its terms the way the device does: each
+// term rounded to a multiple of 2^-64 and added into a 128-bit two's
+// complement integer (order-free, so exact), converted back to FP64 once.
+// The reference's own sum (`total`) is the running FP64 sum below; the two
+// differ only by that sum's rounding, so equality of the fixed-point value
+// with the device's pins the device's cell set and per-cell terms bit for bit.
+struct Fx128 {
+    unsigned long long lo = 0;
+    long long hi = 0;
+    void add(double v)
+    {
+        const double f = std::floor(v);
+        const double frac = v - f;  // exact, in [0, 1)
+        const auto l = static_cast<unsigned long long>(std::nearbyint(frac * 18446744073709551616.0));
+        const unsigned long long sum = lo + l;
+        hi += static_cast<long long>(f) + (sum < l ? 1 : 0);
+        lo = sum;
+    }
+    double value() const
+    {
+        return static_cast<double>(hi) + static_cast<double>(lo) * (1.0 / 18446744073709551616.0);
+    }
+};
+
 double wrap_angle(double a)
 {
     while (a < 0.0) a += 2.0 * kPi;
@@ -1065,6 +1092,8 @@ double polar_impl(const FsSettings& st, const LdTable& ld, double s, double q, P
         enqueue(ir, iphi);
     }
     double total = 0.0;
+    Fx128 fixed;
+    unsigned long long cells = 0;
     while (!queue.empty()) {
         const auto [ir, iphi] = queue.front();
         queue.pop_front();
@@ -1080,9 +1109,17 @@ double polar_impl(const FsSettings& st, const LdTable& ld, double s, double q, P
             const double radius = (static_cast<double>(cur) + 0.5) * dr;
             const double b = ld.uniform ? 1.0 : ld(dz2 * inv_rho2);
             total += b * radius;
+            if (g_polar_fixed) {
+                fixed.add(b * radius);
+                ++cells;
+            }
             enqueue(cur, iphi - 1);
             enqueue(cur, iphi + 1);
         }
+    }
+    if (g_polar_fixed) {
+        g_polar_fixed->value = fixed.value() * dr * dphi / flux;
+        g_polar_fixed->cells = cells;
     }
     return total * dr * dphi / flux;
 }

@@ -66,6 +66,15 @@ std::vector<Pt> seeds(const FsSettings& st, double s, double q, double x, double
 double cartesian(const FsSettings& st, double s, double q, double x, double y, double rho,
                  const std::vector<Pt>& seeds, CartesianDiagnostics* diag);
 
+// The polar integral with its cells summed exactly (a 128-bit fixed-point
+// accumulator with 64 fraction bits, as the device sums them) and how many
+// cells it counted; filled by every polar integration while the pointer is set.
+struct PolarFixedSum {
+    double value = 0.0;
+    unsigned long long cells = 0;
+};
+extern thread_local PolarFixedSum* g_polar_fixed;
+
 // inverse_ray_polar_boundary_binary with given seeds (FSM:1156-1319).
 double polar(const FsSettings& st, double s, double q, double x, double y, double rho, const std::vector<Pt>& seeds);
 

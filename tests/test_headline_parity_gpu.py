@@ -13,9 +13,12 @@ call, as the bench does; the reference (compiled from its own sources,
   lattices: rho near 1e-4 at nbin near 200);
 * 256 random others.
 
-Bar: Cartesian magnifications bit for bit, polar ones within 1e-12 relative
-(the same cell set, summed exactly instead of by the reference's running
-sum), methods equal and status 0 on every point.
+Bar: Cartesian magnifications bit for bit; polar ones within 1e-12 relative
+of the reference (the same cells, summed exactly here and by a running sum
+there), and bit for bit equal, with the same cell count, to the oracle's
+integral of the same lattice with its cells summed the device's way (a
+128-bit fixed-point sum): that pins every polar cell and every cell's term,
+not only the total; methods equal and status 0 on every point.
 """
 import os
 
@@ -80,6 +83,7 @@ def test_headline_batch_subset_matches_reference(ref_lib):
     A = res["magnification"][sel].copy()
     M = res["method"][sel].copy()
     S = res["status"][sel].copy()
+    cells = rays[sel]
     summary = bench.parity_summary(A, M, S, R, RM)
     assert (S == 0).all(), np.unique(S, return_counts=True)
     assert (M == RM).all(), f"{int((M != RM).sum())} methods differ"
@@ -89,6 +93,38 @@ def test_headline_batch_subset_matches_reference(ref_lib):
     assert bad.size == 0, (f"{bad.size} Cartesian points differ, e.g. point {int(sel[bad[0]])}: "
                            f"{A[bad[0]]!r} vs {R[bad[0]]!r}; {summary}")
     pol = M == 3
+    fixed, fcells = _oracle_polar_fixed(rows[sel[pol]])
+    diff = np.nonzero((A[pol].view(np.int64) != fixed.view(np.int64)) | (cells[pol] != fcells))[0]
+    detail = [(int(sel[pol][k]), int(cells[pol][k]), int(fcells[k]), float(A[pol][k] / fixed[k] - 1.0))
+              for k in diff[:8]]
+    assert diff.size == 0, f"{diff.size} polar points differ from the oracle's exact sum (point, cells, oracle cells, rel): {detail}"
     rel = np.abs(A[pol] / R[pol] - 1.0)
     assert rel.max() <= POLAR_REL_TOL, summary
     assert summary["pass"], summary
+
+
+def _oracle_polar_fixed(rows):
+    """The oracle's polar integrals of the rows with the device's exact sum,
+    and their cell counts, one process per core."""
+    import multiprocessing as mp
+    n = max(1, min(len(rows), len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()))
+    with mp.get_context("spawn").Pool(n) as pool:
+        res = pool.map(_fixed_worker, [rows[k::n] for k in range(n)])
+    fixed = np.empty(len(rows))
+    cells = np.empty(len(rows), dtype=np.uint64)
+    for k, (f, c) in enumerate(res):
+        fixed[k::n] = f
+        cells[k::n] = c
+    return fixed, cells
+
+
+def _fixed_worker(rows):
+    from oracle.oracle import Oracle, default_settings
+    orc = Oracle()
+    f, c = [], []
+    for r in rows:
+        st = default_settings(source_bins=int(r[7]), finite_mode=int(r[6]), limb_darkening_c=float(r[5]))
+        _, _, Af, cells = orc.inverse_ray_fixed(st, r[0], r[1], r[2], r[3], r[4])
+        f.append(Af[0])
+        c.append(int(cells[0]))
+    return f, c

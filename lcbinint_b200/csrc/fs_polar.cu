@@ -21,6 +21,7 @@
 // rounding (about 1e-16 relative per term).
 #include "lcbi_fs_kernels.h"
 #include "lcbi_group.cuh"
+#include "lcbi_trig.cuh"
 
 namespace lcbi {
 
@@ -67,7 +68,7 @@ __device__ __forceinline__ Row make_row(const Polar& P, int iphi)
     Row r;
     r.iphi = wrap_phi(P, iphi);
     const double phi = (static_cast<double>(r.iphi) + 0.5) * P.dphi;
-    sincos(phi, &r.sn, &r.cs);
+    trig::sincos_cr(phi, &r.sn, &r.cs);
     return r;
 }
 

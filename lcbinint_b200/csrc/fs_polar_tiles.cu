@@ -24,6 +24,7 @@
 // fit the table is handed to the block flood fill of the second pass.
 #include "lcbi_fs_kernels.h"
 #include "lcbi_group.cuh"
+#include "lcbi_trig.cuh"
 
 #include <cstdint>
 
@@ -212,7 +213,7 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
     double cs = 0.0, sn = 0.0;
     if (valid) {
         const double phi = (static_cast<double>(g) + 0.5) * I.dphi;
-        sincos(phi, &sn, &cs);
+        trig::sincos_cr(phi, &sn, &cs);
     }
     // FP32 rays: one anchor per lattice column of the tile, at its middle radius.
     Anchor32 A{};
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(128) tile_start_kernel(FsWork w, TileCtx G)
                     if (iphi < 0) iphi += I.phi_bins;
                     const double phi = (static_cast<double>(iphi) + 0.5) * I.dphi;
                     double sn, cs;
-                    sincos(phi, &sn, &cs);
+                    trig::sincos_cr(phi, &sn, &cs);
                     if (cell_dz2(I, cs, sn, ir) <= I.rho2) {
                         const double radius = (static_cast<double>(ir) + 0.5) * I.dr;
                         fir = max(0, static_cast<int>(floor(radius / I.dr)));
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(128) tile_start_kernel(FsWork w, TileCtx G)
         {
             const double phi = (static_cast<double>(fiphi) + 0.5) * I.dphi;
             double sn, cs;
-            sincos(phi, &sn, &cs);
+            trig::sincos_cr(phi, &sn, &cs);
             if (!(cell_dz2(I, cs, sn, fir) <= I.rho2)) continue;
         }
         if (fir >= (1 << 30)) {

@@ -90,6 +90,7 @@ bool ensure_scratch(Context* ctx)
 }
 
 size_t cart_bytes_big(const Context* c) { return (cartesian_scratch_bytes(c->row_cap_big, c->seed_cap) + 255) & ~size_t(255); }
+size_t split_bytes(const Context* c) { return (cartesian_scratch_bytes(kSplitRowCap, c->seed_cap) + 255) & ~size_t(255); }
 size_t polar_bytes_big(const Context* c) { return (polar_scratch_bytes(c->queue_cap_big, c->hash_cap_big) + 255) & ~size_t(255); }
 
 int retry_blocks(const Context* c) { return c->retry_blocks > 0 ? c->retry_blocks : c->sm_count; }
@@ -100,9 +101,14 @@ bool ensure_big_scratch(Context* ctx)
     // Cartesian: the second pass's blocks, then kEarlyMax blocks of the early pass.
     const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + kEarlyMax);
     const size_t pb = polar_bytes_big(ctx) * retry_blocks(ctx);
-    if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb)) return false;
+    // The units of the split early points: one small row scratch each.
+    const size_t sb = split_bytes(ctx) * kSplitUnits;
+    if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb) ||
+        !ctx->ensure(ctx->fs_split, sb) || !ctx->ensure(ctx->fs_split_info, kSplitUnits * sizeof(SplitInfo)))
+        return false;
     if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_big.ptr, 0xff, cb, ctx->stream)) ||
-        !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar_big.ptr, 0xff, pb, ctx->stream)))
+        !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar_big.ptr, 0xff, pb, ctx->stream)) ||
+        !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_split.ptr, 0xff, sb, ctx->stream)))
         return false;
     ctx->big_ready = true;
     return true;
@@ -302,7 +308,7 @@ void set_lists(FsWork& w, int* counters, int* lists, int* retry, long long cap_c
 // The decision of every point of w (work lists and counters reset first).
 bool stage_decide(Context* ctx, const FsWork& w)
 {
-    if (!ctx->check("counters", cudaMemsetAsync(w.ir_count, 0, 64 * sizeof(int), ctx->stream))) return false;
+    if (!ctx->check("counters", cudaMemsetAsync(w.ir_count, 0, kCounterInts * sizeof(int), ctx->stream))) return false;
     cudaEvent_t ev;
     ctx->stage_begin(1, &ev);
     if (!ctx->check("decide", launch_decide(w, ctx->sm_count, ctx->stream))) return false;
@@ -346,6 +352,9 @@ FsWork early_work(Context* ctx, const FsWork& w)
                 (long long)retry_blocks(ctx) * static_cast<long long>(cart_bytes_big(ctx));
     e.scratch_per_warp = static_cast<long long>(cart_bytes_big(ctx));
     e.row_cap = ctx->row_cap_big;
+    e.split_scratch = static_cast<char*>(ctx->fs_split.ptr);
+    e.split_bytes = static_cast<long long>(split_bytes(ctx));
+    e.split_info = static_cast<SplitInfo*>(ctx->fs_split_info.ptr);
     return e;
 }
 
@@ -387,7 +396,7 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
             const bool ok =
                 ctx->check("seeds early", launch_seeds(es, ctx->sm_count, ctx->early_stream, ek, ep, kEarlyMax)) &&
                 ctx->check("cartesian early",
-                           launch_cartesian(early_work(ctx, w), kEarlyMax, ctx->early_stream, ctx->epoch));
+                           launch_cartesian(early_work(ctx, w), kEarlyBlocks, ctx->early_stream, ctx->epoch));
             // Recorded even after a failed launch: the context's stream must
             // never run ahead of work already queued beside it.
             if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream))) return false;
@@ -432,7 +441,7 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     if (ctx->early_serial) {
         // Stage timing on: the early block pass (stage_seeds) runs here, first.
         ctx->stage_begin(3, &ev);
-        if (!ctx->check("cartesian early", launch_cartesian(early_work(ctx, w), kEarlyMax, ctx->stream, ctx->epoch)))
+        if (!ctx->check("cartesian early", launch_cartesian(early_work(ctx, w), kEarlyBlocks, ctx->stream, ctx->epoch)))
             return false;
         ctx->stage_end(3, ev);
     }
@@ -514,7 +523,7 @@ bool prepare_tables(Context* ctx, const Plan& plan)
         !upload(ctx, ctx->fs_raw_offset, plan.raw_offset) || !upload(ctx, ctx->fs_phases, plan.phases) ||
         !upload(ctx, ctx->fs_ld_coeffs, plan.ld_coeffs) ||
         !ctx->ensure(ctx->fs_ld, (size_t)(nld + 1) * (kLdTable + 1) * sizeof(double)) ||
-        !ctx->ensure(ctx->fs_counters, 64 * sizeof(int)))
+        !ctx->ensure(ctx->fs_counters, kCounterInts * sizeof(int)))
         return false;
     if (ctx->tile_blocks == 0) ctx->tile_blocks = polar_tile_blocks_per_sm() * ctx->sm_count;
     // Adaptive local refinement needs a tape per scratch group.
@@ -1125,7 +1134,7 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
         if (!ctx->ensure(ctx->pass_raw[k], (max_raw + 1) * sizeof(P2)) ||
             !ctx->ensure(ctx->pass_branches[k], (max_raw + 1) * sizeof(P2)) ||
             !ctx->ensure(ctx->pass_lists[k], list_ints * sizeof(int)) ||
-            !ctx->ensure(ctx->pass_counters[k], 64 * sizeof(int)) || !ctx->ensure(ctx->pass_jobs[k], job_bytes))
+            !ctx->ensure(ctx->pass_counters[k], kCounterInts * sizeof(int)) || !ctx->ensure(ctx->pass_jobs[k], job_bytes))
             return LCBI_GPU_ERROR;
     }
     if (ctx->pinned_bytes < 2 * stage_bytes) {
@@ -1244,7 +1253,7 @@ int binary_mag_images(lcbi_gpu_context* c, const lcbi_fs_settings* settings, int
     if (n_ir > 0) {
         std::vector<int> lists(g_cart);
         lists.insert(lists.end(), g_polar.begin(), g_polar.end());
-        std::vector<int> counters(64, 0);
+        std::vector<int> counters(kCounterInts, 0);
         counters[0] = n_cart;
         counters[1] = n_polar;
         if (!upload(ctx, ctx->ir_lists, lists) || !upload(ctx, ctx->ir_counters, counters) ||

@@ -304,7 +304,8 @@ __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a,
     return acc;
 }
 
-// cartesian_image_area_impl: one directional flood fill from `seed`.
+// cartesian_image_area_impl: one directional flood fill from `seed`
+// (with stop_rows > 0, only until that many rows have completed).
 //
 // Every thread runs the same state machine on the same values, so the row
 // bounds the scan needs again (the previous row's xmin and xmax, the current
@@ -313,7 +314,8 @@ __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a,
 // row-key table slot of each row is fetched when the row starts, so its load
 // overlaps the row's lens-map evaluations.
 template <int W>
-__device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, double dy, int& yi, int jsign)
+__device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, double dy, int& yi, int jsign,
+                             int stop_rows = 0)
 {
     constexpr int N = Grp<W>::N;
     double countx = 0.0, countall = 0.0, dz2 = 99999999.9;
@@ -492,6 +494,8 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                                                        (unsigned long long)(unsigned)(yi + 1));
             if (Grp<W>::rank() == 0) R.next[yi] = head;
             ++yi;
+            // A split point's down unit needs only the up scan's first row.
+            if (stop_rows > 0 && yi >= stop_rows) return countall;
             rows_ensure<W>(R, yi);
             if (R.ovf) return countall;
             dx = incr;
@@ -763,6 +767,158 @@ __device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, doubl
     return out;
 }
 
+// The row scratch at `base` (cartesian_scratch_bytes(cap, seed_cap) bytes):
+// five row arrays and the per-seed areas (doubles), the row-key table
+// (16-byte entries), then the row chains and the per-seed flags (ints).
+__device__ __forceinline__ RowScratch rows_at(char* base, int cap, int seed_cap, double** areaimage, int** flags)
+{
+    RowScratch R;
+    R.xmin = reinterpret_cast<double*>(base);
+    R.xmax = R.xmin + cap;
+    R.ax = R.xmax + cap;
+    R.y = R.ax + cap;
+    R.dys = R.y + cap;
+    double* ai = R.dys + cap;
+    R.table = reinterpret_cast<ulonglong2*>((reinterpret_cast<uintptr_t>(ai + seed_cap) + 15) &
+                                            ~static_cast<uintptr_t>(15));
+    R.tmask = (unsigned)table_slots(cap) - 1u;
+    R.next = reinterpret_cast<int*>(R.table + table_slots(cap));
+    R.cap = cap;
+    R.hw = 0;
+    R.gen = 0;
+    R.ovf = false;
+    if (areaimage) *areaimage = ai;
+    if (flags) *flags = R.next + cap + 2;  // per seed: bit0 overlapped (skip), bit1 subtracted
+    return R;
+}
+
+// The units of a split early point: seed ii's up scan is unit 2 ii, its down
+// scan unit 2 ii + 1, each with a SplitInfo and a kSplitRowCap-row scratch.
+struct SplitUse {
+    const SplitInfo* info;
+    char* scratch;
+    long long bytes;
+    int seed_cap;
+};
+
+__device__ __forceinline__ SplitInfo load_info(const SplitInfo* p)
+{
+    SplitInfo v;
+    v.area = __ldcg(&p->area);
+    v.rays = __ldcg(&p->rays);
+    v.yi_final = __ldcg(&p->yi_final);
+    v.pred = __ldcg(&p->pred);
+    v.ok = __ldcg(&p->ok);
+    v.pad = 0;
+    for (int i = 0; i < 3; ++i) v.row0[i] = __ldcg(&p->row0[i]);
+    return v;
+}
+
+__device__ __forceinline__ bool same_bits(double a, double b)
+{
+    return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// Seed ii's two directional scans taken from its units instead of run here:
+// R receives the up scan's rows, the predecessor row the down scan starts
+// from, then the down scan's rows, at the indices one scan of the seed
+// gives them, and yi, areai and the cell count follow as after the two
+// scans (the caller sets R.hw, yi, areai and the cells from the result).
+// The two scans of one seed are independent: the down scan reads
+// the first row's bounds (its unit scans that row itself and stops) and
+// rows of its own row keys, and every down-scan row lies below every up-scan
+// row, so when the down scan's first key is below the up scan's first key
+// (keys grow with y) no key is shared.  The rows are not yet in the row-key
+// table: fill_table enters them when a gap repair is about to read it, and
+// n_up is the up scan's row count for that.  ok = false, with R untouched:
+// a unit did not fit its rows, the keys could meet, or the merged rows would
+// not fit R; the seed is then scanned here.
+struct MergeOut {
+    bool ok;
+    int yi, n_up, hw;
+    double areai;
+    unsigned long long rays;
+};
+
+template <int W>
+__device__ __noinline__ MergeOut merge_halves(RowScratch R, SplitUse sp, int ii, P2 seed, double incr)
+{
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
+    MergeOut m{false, 0, 0, 0, 0.0, 0ull};
+    const SplitInfo U = load_info(sp.info + 2 * ii);
+    const SplitInfo D = load_info(sp.info + 2 * ii + 1);
+    if (!U.ok || !D.ok) return m;
+    const double inv_incr = 1.0 / incr;
+    if (!(row_key(seed.y + (-incr), inv_incr) < row_key(seed.y, inv_incr))) return m;
+    const RowScratch UR = rows_at(sp.scratch + (long long)(2 * ii) * sp.bytes, kSplitRowCap, sp.seed_cap, nullptr,
+                                  nullptr);
+    const RowScratch DR = rows_at(sp.scratch + (long long)(2 * ii + 1) * sp.bytes, kSplitRowCap, sp.seed_cap,
+                                  nullptr, nullptr);
+    const int nu = U.yi_final;
+    if (D.pred != (nu > 0 ? 1 : 0)) return m;
+    const double x0m = __ldcg(UR.xmin), x0M = __ldcg(UR.xmax), y0 = __ldcg(UR.y);
+    if (!same_bits(D.row0[0], x0m) || !same_bits(D.row0[1], x0M) || !same_bits(D.row0[2], y0)) return m;
+    const int total = nu + (D.yi_final - D.pred);
+    if (total + 1 > R.cap) return m;
+    for (int r = t; r <= total; r += N) {
+        const bool up = r <= nu;
+        const RowScratch& Q = up ? UR : DR;
+        const int q = up ? r : D.pred + (r - nu);
+        R.xmin[r] = __ldcg(Q.xmin + q);
+        R.xmax[r] = __ldcg(Q.xmax + q);
+        R.ax[r] = __ldcg(Q.ax + q);
+        R.y[r] = __ldcg(Q.y + q);
+        R.dys[r] = __ldcg(Q.dys + q);
+    }
+    Grp<W>::sync();
+    // The predecessor row: the first row's bounds and y, direction down (its
+    // ax stays what the up scan left at that index).
+    if (t == 0) {
+        R.xmin[nu] = x0m;
+        R.xmax[nu] = x0M;
+        R.y[nu] = y0;
+        R.dys[nu] = -incr;
+    }
+    Grp<W>::sync();
+    m.ok = true;
+    m.yi = total;
+    m.n_up = nu;
+    m.hw = total + 1;
+    m.areai = U.area;
+    m.areai += D.area;
+    m.rays = U.rays + D.rays;
+    return m;
+}
+
+// Enters a merged seed's rows into the row-key table in row order, as its
+// two scans would have: rows [0, n_up) and (n_up, yi) (the predecessor row
+// and the down scan's last row never get an entry).  By rank 0, then a
+// barrier; true (in every thread) when the table is full.
+template <int W>
+__device__ __noinline__ bool fill_table(RowScratch R, int n_up, int yi, double incr)
+{
+    bool full = false;
+    if (Grp<W>::rank() == 0) {
+        const double inv_incr = 1.0 / incr;
+        for (int r = 0; r < yi; ++r) {
+            if (r == n_up) continue;
+            const int key = row_key(R.y[r], inv_incr);
+            unsigned slot;
+            const int e = key_lookup(R, key, &slot);
+            if (slot == 0xffffffffu) {
+                full = true;
+                break;
+            }
+            R.next[r] = e;
+            R.table[slot] = make_ulonglong2(R.gen, ((unsigned long long)(unsigned)key << 32) |
+                                                       (unsigned long long)(unsigned)(r + 1));
+        }
+    }
+    Grp<W>::sync();
+    return Grp<W>::any(full);
+}
+
 // One scan of a point's lattice (inverse_ray_cartesian_binary_mag,
 // FSM:2470-2768) at `source_bins` cells per source radius: the directional
 // flood fills of every seed that no earlier seed's rows cover, their gap
@@ -772,7 +928,7 @@ __device__ Refined refine(const Ctx& C, const FsSettingsDev& st, double A, doubl
 template <int W>
 __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* seeds, int ns, double rho,
                            int source_bins, unsigned long long epoch, unsigned long long& local_gen,
-                           double* areaimage, int* flags, Diag& d, double& area)
+                           double* areaimage, int* flags, Diag& d, double& area, const SplitUse* sp = nullptr)
 {
     constexpr int N = Grp<W>::N;
     const int t = Grp<W>::rank();
@@ -806,30 +962,49 @@ __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* se
         const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
         ++d.processed;
         if (js != 0) ++d.fold;
-        wset<W>(R.xmin, 0, seed.x);
-        wset<W>(R.xmax, 0, seed.x);
-        Grp<W>::sync();
-        areai = image_area<W>(C, R, S, seed, dy, yi, js);
-        Grp<W>::sync();
-        dy = -incr;
-        rows_ensure<W>(R, yi);
-        if (R.ovf) {
-            ovf = true;
-            break;
-        }
-        const P2 lower{R.xmax[0], seed.y + dy};
-        {
-            const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
+        // n_up >= 0: the two scans came from the seed's split units, and their
+        // rows enter the row-key table before the first gap repair.
+        int n_up = -1;
+        MergeOut mo{false, 0, 0, 0, 0.0, 0ull};
+        if (sp != nullptr && ii < kSplitSeeds) mo = merge_halves<W>(R, *sp, ii, seed, incr);
+        if (mo.ok) {
+            yi = mo.yi;
+            n_up = mo.n_up;
+            R.hw = mo.hw;
+            areai = mo.areai;
+            C.rays += mo.rays;
+        } else {
+            wset<W>(R.xmin, 0, seed.x);
+            wset<W>(R.xmax, 0, seed.x);
             Grp<W>::sync();
-            wset<W>(R.xmin, yi, xm0);
-            wset<W>(R.xmax, yi, xM0);
-            wset<W>(R.y, yi, y0);
-            wset<W>(R.dys, yi, dy);
+            areai = image_area<W>(C, R, S, seed, dy, yi, js);
+            Grp<W>::sync();
+            dy = -incr;
+            rows_ensure<W>(R, yi);
+            if (R.ovf) {
+                ovf = true;
+                break;
+            }
+            const P2 lower{R.xmax[0], seed.y + dy};
+            {
+                const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
+                Grp<W>::sync();
+                wset<W>(R.xmin, yi, xm0);
+                wset<W>(R.xmax, yi, xM0);
+                wset<W>(R.y, yi, y0);
+                wset<W>(R.dys, yi, dy);
+                Grp<W>::sync();
+            }
+            ++yi;
+            areai += image_area<W>(C, R, S, lower, dy, yi, js);
             Grp<W>::sync();
         }
-        ++yi;
-        areai += image_area<W>(C, R, S, lower, dy, yi, js);
-        Grp<W>::sync();
+        auto table_ready = [&]() {
+            if (n_up >= 0) {
+                if (fill_table<W>(R, n_up, yi, incr)) R.ovf = true;
+                n_up = -1;
+            }
+        };
         int nyi = yi;
         double areabound = 0.0;
         for (int row = 0; row < nyi && !R.ovf; ++row) {
@@ -840,21 +1015,25 @@ __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* se
             if (R.ax[row + 1] > 0.0) {
                 if (dxmax > 1.1 * incr) {
                     ++d.gap_repairs;
+                    table_ready();
                     repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1],
                               -R.dys[row], yi, js, areai, areabound);
                 }
                 if (dxmin > 1.1 * incr) {
                     ++d.gap_repairs;
+                    table_ready();
                     repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row],
                               R.xmin[row + 1], R.dys[row], yi, js, areai, areabound);
                 }
                 if (dxmin < -1.1 * incr) {
                     ++d.gap_repairs;
+                    table_ready();
                     repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row],
                               -R.dys[row], yi, js, areai, areabound);
                 }
                 if (dxmax < -1.1 * incr) {
                     ++d.gap_repairs;
+                    table_ready();
                     repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1],
                               R.xmax[row], R.dys[row], yi, js, areai, areabound);
                 }
@@ -930,38 +1109,204 @@ struct CartList {
     int* next;          // dynamic work counter
 };
 
+// The per-point state of a scan (cartesian_body, run_unit): the point's lens
+// map, source and limb-darkening table (copied to ld_smem, when given, once
+// per table), and the scan limits.
+template <int W>
+__device__ void init_ctx(Ctx& C, const FsWork& w, const FsItem& item, const FsSettingsDev& st, TapeCell* tape,
+                         double* ld_smem, int& ld_loaded)
+{
+    const int t = Grp<W>::rank();
+    const double rho = item.rho;
+    C.m = make_mapper(item.s, item.q);
+    C.src = P2{item.x, item.y};
+    C.rho = rho;
+    C.rho2 = rho * rho;
+    C.inv_rho2 = 1.0 / C.rho2;
+    C.uniform = st.ld_c == 0.0 && st.ld_d == 0.0;
+    // I(r^2) >= 1 - c - d on [0, 1] for c, d >= 0, so every counted cell adds > 0.
+    C.bulk = C.uniform || (st.ld_c >= 0.0 && st.ld_d >= 0.0 && st.ld_c + st.ld_d < 1.0);
+    C.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
+    C.lds = nullptr;
+    if (ld_smem != nullptr && !C.uniform) {
+        // A block scan keeps its point's table in shared memory: the
+        // brightness lookup ends every cell's evaluation.
+        if (ld_loaded != st.ld_table) {
+            Grp<W>::sync();
+            for (int i = t; i <= kLdTable; i += Grp<W>::N) ld_smem[i] = C.ld[i];
+            Grp<W>::sync();
+            ld_loaded = st.ld_table;
+        }
+        C.lds = ld_smem;
+    }
+    C.max_steps = max(100000, st.source_bins * st.source_bins * 2000);
+    C.f32 = w.f32_rays != 0;
+    // Adaptive local refinement records the scan's boundary cells, so
+    // every cell goes through the reference's loop body (no bulk runs).
+    const bool adaptive = tape && st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0);
+    C.tape = adaptive ? tape : nullptr;
+    C.tape_max = max(64, st.max_source_bins);
+    if (C.tape_max > kTapeMax) C.tape_max = kTapeMax;
+    if (adaptive) C.bulk = false;
+}
+
+// One unit of a split early point (early point e, seed ii, half 0 up or 1
+// down): the seed's directional scan at the point's source_bins into the
+// unit's own scratch, exactly as scan_point runs it (the down half first
+// scans the up scan's first row itself, for the bounds it starts from, and
+// counts only its own cells).  The result goes to the unit's SplitInfo; a
+// missing point or seed, or a scan that outgrows the unit's rows, leaves
+// ok = 0 and the finishing block scans that seed itself.
+struct UnitArgs {
+    const int* early_cart;
+    const int* ir_cart;
+    const FsItem* items;
+    const FsOut* out;
+    const FsSettingsDev* settings;
+    const double* ld_tables;
+    const P2* seeds;
+    char* split_scratch;
+    SplitInfo* split_info;
+    long long split_bytes;
+    int seed_cap;
+    int f32_rays;
+};
+
+template <int W>
+__device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e, int ii, int half, CartShared<W>& S,
+                                     double* ld_smem, int ld_loaded)
+{
+    const int u = (e * kSplitSeeds + ii) * 2 + half;
+    SplitInfo info{};
+    const int k = w.early_cart[e];
+    const int it = w.ir_cart[k];
+    const FsItem item = w.items[it];
+    const FsOut o = w.out[it];
+    if (o.status == kFsOk && ii < o.n_seeds && item.rho > 0.0) {
+        const FsSettingsDev st = w.settings[item.settings];
+        Ctx C;
+        C.rays = 0;
+        C.evals = 0;
+        C.budget = 0;
+        FsWork lw{};
+        lw.ld_tables = w.ld_tables;
+        lw.f32_rays = w.f32_rays;
+        init_ctx<W>(C, lw, item, st, nullptr, ld_smem, ld_loaded);
+        RowScratch R = rows_at(w.split_scratch + (long long)u * w.split_bytes, kSplitRowCap, w.seed_cap, nullptr,
+                               nullptr);
+        R.gen = (epoch << 32) | 1ull;
+        const double incr = item.rho / static_cast<double>(max(st.source_bins, 1));
+        C.band = dmax_(4.0 * item.rho * incr, 4.0 * incr * incr);
+        C.step = incr;
+        C.tape_n = 0;
+        rows_ensure<W>(R, 1);
+        const P2 seed = w.seeds[(long long)k * w.seed_cap + ii];
+        if (C.f32) C.A = make_anchor32(C.m, seed.x, seed.y, C.src);
+        const double jseed = jacobian(C.m, seed.x, seed.y);
+        const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
+        wset<W>(R.xmin, 0, seed.x);
+        wset<W>(R.xmax, 0, seed.x);
+        Grp<W>::sync();
+        int yi = 0;
+        if (half == 0) {
+            info.area = image_area<W>(C, R, S, seed, incr, yi, js);
+            Grp<W>::sync();
+            rows_ensure<W>(R, yi);
+            info.yi_final = yi;
+            info.rays = C.rays;
+        } else {
+            image_area<W>(C, R, S, seed, incr, yi, js, 1);
+            Grp<W>::sync();
+            const unsigned long long rays0 = C.rays;
+            rows_ensure<W>(R, yi);
+            if (!R.ovf) {
+                const double dy = -incr;
+                const double xm0 = R.xmin[0], xM0 = R.xmax[0], y0 = R.y[0];
+                info.row0[0] = xm0;
+                info.row0[1] = xM0;
+                info.row0[2] = y0;
+                const P2 lower{xM0, seed.y + dy};
+                Grp<W>::sync();
+                wset<W>(R.xmin, yi, xm0);
+                wset<W>(R.xmax, yi, xM0);
+                wset<W>(R.y, yi, y0);
+                wset<W>(R.dys, yi, dy);
+                Grp<W>::sync();
+                info.pred = yi;
+                ++yi;
+                info.area = image_area<W>(C, R, S, lower, dy, yi, js);
+                Grp<W>::sync();
+                rows_ensure<W>(R, yi);
+                info.yi_final = yi;
+                info.rays = C.rays - rays0;
+            }
+        }
+        info.ok = R.ovf ? 0 : 1;
+    }
+    if (Grp<W>::rank() == 0) w.split_info[u] = info;
+    return ld_loaded;
+}
+
+// Work items: the list's points in order, each with the scratch at `base`.
+// The early pass with split points (split_info set) takes first the units of
+// its first kSplitPoints points, kSplitSeeds seeds by two halves each, then
+// its other points; a point's scratch is the early pass's area at its list
+// position, and the block whose unit completes a split point's last unit
+// finishes that point from the units' rows (the units of a point run on
+// other blocks at the same time, so its scans take the time of the longest
+// half instead of the sum of all).
 template <int W>
 __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S,
                                TapeCell* tape, double* ld_smem = nullptr)
 {
     int ld_loaded = -1;  // the limb-darkening table now in ld_smem
-    constexpr int N = Grp<W>::N;
     const int t = Grp<W>::rank();
     const int cap = w.row_cap;
-    RowScratch R;
-    R.xmin = reinterpret_cast<double*>(base);
-    R.xmax = R.xmin + cap;
-    R.ax = R.xmax + cap;
-    R.y = R.ax + cap;
-    R.dys = R.y + cap;
-    // Layout, every array aligned: five row arrays and the per-seed areas
-    // (doubles), the row-key table (16-byte entries), then the int arrays.
-    double* areaimage = R.dys + cap;
-    R.table = reinterpret_cast<ulonglong2*>((reinterpret_cast<uintptr_t>(areaimage + w.seed_cap) + 15) &
-                                            ~static_cast<uintptr_t>(15));
-    R.tmask = (unsigned)table_slots(cap) - 1u;
-    R.next = reinterpret_cast<int*>(R.table + table_slots(cap));
-    int* flags = R.next + cap + 2;  // per seed: bit0 overlapped (skip), bit1 subtracted
-    R.cap = cap;
+    double* areaimage;
+    int* flags;
+    RowScratch R = rows_at(base, cap, w.seed_cap, &areaimage, &flags);
     unsigned long long local_gen = 0;
     const int n = *L.count;
+    const bool split = w.early_pass && w.split_info != nullptr && L.slots != nullptr;
+    const int n_split = split ? min(n, kSplitPoints) : 0;
+    const int n_units = n_split * 2 * kSplitSeeds;
+    const int n_work = split ? n_units + (n - n_split) : n;
     for (;;) {
         Grp<W>::sync();
         if (t == 0) S.item = atomicAdd(L.next, 1);
         Grp<W>::sync();
-        int k = S.item;
-        if (k >= n) break;
-        if (L.slots) k = L.slots[k];
+        const int idx = S.item;
+        if (idx >= n_work) break;
+        int k = idx;
+        int e = idx;  // early pass: the point's list position
+        SplitUse su{nullptr, nullptr, 0, 0};
+        const SplitUse* use = nullptr;
+        if (split) {
+            if (idx < n_units) {
+                e = idx / (2 * kSplitSeeds);
+                const UnitArgs ua{w.early_cart, w.ir_cart, w.items, w.out, w.settings, w.ld_tables, w.seeds,
+                                  w.split_scratch, w.split_info, w.split_bytes, w.seed_cap, w.f32_rays};
+                ld_loaded = run_unit<W>(ua, epoch, e, (idx >> 1) % kSplitSeeds, idx & 1, S, ld_smem, ld_loaded);
+                __threadfence();
+                Grp<W>::sync();
+                if (t == 0) S.item = atomicAdd(w.ir_count + kSplitCounter + e, 1);
+                Grp<W>::sync();
+                if (S.item != 2 * kSplitSeeds - 1) continue;
+                __threadfence();
+                su = SplitUse{w.split_info + (long long)e * 2 * kSplitSeeds,
+                              w.split_scratch + (long long)e * 2 * kSplitSeeds * w.split_bytes, w.split_bytes,
+                              w.seed_cap};
+                use = &su;
+            } else {
+                e = n_split + (idx - n_units);
+            }
+        }
+        if (w.early_pass) {
+            k = L.slots[e];
+            R = rows_at(w.scratch + (long long)e * w.scratch_per_warp, cap, w.seed_cap, &areaimage, &flags);
+        } else if (L.slots) {
+            k = L.slots[k];
+        }
         if (W == 1 && !w.retry_pass && w.early_cart != nullptr) {
             // Points routed to the early block pass are not run here.
             const int ne = w.ir_count[5];
@@ -985,36 +1330,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         C.evals = 0;
         C.budget = (W == 1 && !w.retry_pass) ? (n <= w.few_points ? 1 : w.cell_budget) : 0;
         if (ns > 0 && rho > 0.0) {
-            C.m = make_mapper(item.s, item.q);
-            C.src = P2{item.x, item.y};
-            C.rho = rho;
-            C.rho2 = rho * rho;
-            C.inv_rho2 = 1.0 / C.rho2;
-            C.uniform = st.ld_c == 0.0 && st.ld_d == 0.0;
-            // I(r^2) >= 1 - c - d on [0, 1] for c, d >= 0, so every counted cell adds > 0.
-            C.bulk = C.uniform || (st.ld_c >= 0.0 && st.ld_d >= 0.0 && st.ld_c + st.ld_d < 1.0);
-            C.ld = w.ld_tables + (long long)st.ld_table * (kLdTable + 1);
-            C.lds = nullptr;
-            if (ld_smem != nullptr && !C.uniform) {
-                // A block scan keeps its point's table in shared memory: the
-                // brightness lookup ends every cell's evaluation.
-                if (ld_loaded != st.ld_table) {
-                    Grp<W>::sync();
-                    for (int i = t; i <= kLdTable; i += Grp<W>::N) ld_smem[i] = C.ld[i];
-                    Grp<W>::sync();
-                    ld_loaded = st.ld_table;
-                }
-                C.lds = ld_smem;
-            }
-            C.max_steps = max(100000, st.source_bins * st.source_bins * 2000);
-            C.f32 = w.f32_rays != 0;
-            // Adaptive local refinement records the scan's boundary cells, so
-            // every cell goes through the reference's loop body (no bulk runs).
-            const bool adaptive = tape && st.adaptive_source_bins != 0 && (st.tol > 0.0 || st.reltol > 0.0);
-            C.tape = adaptive ? tape : nullptr;
-            C.tape_max = max(64, st.max_source_bins);
-            if (C.tape_max > kTapeMax) C.tape_max = kTapeMax;
-            if (adaptive) C.bulk = false;
+            init_ctx<W>(C, w, item, st, tape, ld_smem, ld_loaded);
             // The scan, and the topology retry of fixed_inverse_ray_binary
             // (FSM:3168-3196): when needs_global_topology_retry (FSM:1108-1121)
             // holds, the same seeds are scanned again at
@@ -1030,7 +1346,8 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
             for (int attempt = 0;; ++attempt) {
                 Diag d{ns, 0, 0, 0, 0, 0, 0.0};
                 double area = 0.0;
-                ovf = scan_point<W>(C, R, S, seeds, ns, rho, bins, epoch, local_gen, areaimage, flags, d, area);
+                ovf = scan_point<W>(C, R, S, seeds, ns, rho, bins, epoch, local_gen, areaimage, flags, d, area,
+                                    attempt == 0 ? use : nullptr);
                 if (ovf) break;
                 const double nb = static_cast<double>(max(bins, 1));
                 const double flux = source_flux(rho, st.ld_c, st.ld_d);
@@ -1119,7 +1436,9 @@ __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWo
     extern __shared__ double ld_smem[];
     const CartList L = w.early_pass ? CartList{w.early_cart, w.ir_count + 5, w.next_item + 6}
                                     : CartList{w.retry_cart, w.ir_count + 2, w.next_item + 3};
-    cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
+    // The early pass takes its scratch by list position (cartesian_body).
+    char* base = w.early_pass ? w.scratch : w.scratch + (long long)blockIdx.x * w.scratch_per_warp;
+    cartesian_body<kBigWarps>(w, epoch, L, base, sh,
                               w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr, ld_smem);
 }
 

@@ -137,9 +137,37 @@ struct FsWork {
     // pass, which has no such waits.
     unsigned wait_limit;
     int* wait_timeouts;
+    // Early points split into units (early pass only; split_info null: off):
+    // the up and the down scan of each of the first kSplitSeeds seeds of the
+    // first kSplitPoints early points run as separate work items, each on its
+    // own block and its own kSplitRowCap-row scratch (split_bytes each at
+    // split_scratch, unit u = (point * kSplitSeeds + seed) * 2 + half), and the
+    // block that completes a point's last unit (the point's counter at
+    // ir_count[kSplitCounter + point]) finishes the point from their rows.
+    char* split_scratch;
+    long long split_bytes;
+    struct SplitInfo* split_info;
 };
 
 constexpr int kEarlyMax = 32;
+
+// One unit of a split early point: what its half scan left.
+struct SplitInfo {
+    double area;              // the half's image_area value
+    unsigned long long rays;  // its inside cells
+    int yi_final;             // the scan's row index when it returned
+    int pred;                 // down half: index of the predecessor row (rows the first row's scan completed)
+    int ok;                   // 1: the point, seed and scan exist and fit the unit's rows
+    int pad;
+    double row0[3];           // down half: xmin, xmax and y of the first row of the up scan
+};
+constexpr int kSplitPoints = 16;
+constexpr int kSplitSeeds = 4;
+constexpr int kSplitUnits = kSplitPoints * kSplitSeeds * 2;
+constexpr int kSplitRowCap = 65536;
+constexpr int kSplitCounter = 64;  // ir_count[64, 64 + kSplitPoints): completed units per split point
+constexpr int kCounterInts = 128;  // size of the counters array (ir_count, next_item, early_cart, ...)
+constexpr int kEarlyBlocks = 96;   // blocks of the early pass
 
 constexpr int kBigWarps = 8;
 

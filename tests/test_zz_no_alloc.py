@@ -159,12 +159,12 @@ def test_noalloc_rings_past_the_fixed_limits_get_status_18_and_19():
     _lib_mod, L = _lib()
     ctx = _lib_mod.Context(0)
     try:
-        # Cartesian: a ring of rho = 2e-4 at 30 bins has more than 65,536 rows
-        # per seed scan (each direction stops at the reference's step cap of
-        # 2000 nbin^2 cells, about 56,000 rows); polar: rho = 1e-4 at 20 bins
-        # has about 314,000 azimuthal rows of segments, past 262,144 slots.
-        for mode, rho_big, status in ((1, 2e-4, 18), (2, 1e-4, 19)):
-            st = _settings(mode, 0.4, bins=30 if mode == 1 else 20)
+        # Cartesian: a ring of rho = 2e-3 at 80 bins has about 85,000 rows in
+        # one seed's scans (the oracle's count), past 65,536; polar: rho = 1e-4
+        # at 20 bins has about 314,000 azimuthal rows of segments, past
+        # 262,144 slots.
+        for mode, rho_big, status in ((1, 2e-3, 18), (2, 1e-4, 19)):
+            st = _settings(mode, 0.4, bins=80 if mode == 1 else 20)
             y1, y2, rho = _ring_points([rho_big], 40, seed=mode)
             ref = _workspace(ctx, L, st, *RING, y1, y2, rho)
             assert ref["status"][0] == 0 and np.isfinite(ref["magnification"][0])

@@ -98,11 +98,11 @@ int retry_blocks(const Context* c) { return c->retry_blocks > 0 ? c->retry_block
 bool ensure_big_scratch(Context* ctx)
 {
     if (ctx->big_ready) return true;
-    // Cartesian: the second pass's blocks, then kEarlyMax blocks of the early pass.
-    const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + kEarlyMax);
+    // Cartesian: the second pass's blocks, then the early pass's blocks.
+    const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + kEarlyBlocks);
     const size_t pb = polar_bytes_big(ctx) * retry_blocks(ctx);
     // The units of the split early points: one small row scratch each.
-    const size_t sb = split_bytes(ctx) * kSplitUnits;
+    const size_t sb = split_bytes(ctx) * kSplitSlots;
     if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb) ||
         !ctx->ensure(ctx->fs_split, sb) || !ctx->ensure(ctx->fs_split_info, kSplitUnits * sizeof(SplitInfo)))
         return false;
@@ -302,7 +302,7 @@ void set_lists(FsWork& w, int* counters, int* lists, int* retry, long long cap_c
     w.retry_cart = retry;
     w.retry_polar = retry + cap_retry;
     w.retry_seeds = retry ? retry + 2 * cap_retry : nullptr;
-    w.early_cart = counters + 16;  // counters[16, 16 + kEarlyMax); the candidate count is counters[48]
+    w.early_cart = counters + kEarlyOff;  // the layout: lcbi_fs_kernels.h
 }
 
 // The decision of every point of w (work lists and counters reset first).
@@ -332,12 +332,15 @@ bool next_epoch(Context* ctx)
     return true;
 }
 
-// Cartesian points predicted to pass the first pass's cell budget four times
-// over or more would spend the whole budget on their warp before starting
-// again on a block after the first pass.  They run on blocks from the start
-// instead (largest first, at most kEarlyMax, with their own scratch blocks
-// after the second pass's); the first pass skips them.  Adaptive refinement
-// keeps one tape per group and does not use this path.
+// Cartesian points predicted to count more than half the first pass's cell
+// budget (pi nbin^2 max(|A_ps|, 1) cells) would often spend the whole budget
+// on their warp before starting again on a block after the first pass, and
+// a point of a few million cells on one block sets the step.  They run on
+// blocks from the start instead, largest first, at most kEarlyMax, each
+// seed's two directional scans as units on blocks of their own (the early
+// pass's blocks have their own scratch after the second pass's); the first
+// pass skips them.  Adaptive refinement keeps one tape per group and does
+// not use this path.
 bool early_routing(const Context* ctx, const FsWork& w)
 {
     return ctx->cell_budget > 0 && w.tape == nullptr && w.early_cart != nullptr;
@@ -378,7 +381,7 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
     cudaEvent_t ev;
     const bool early = early_routing(ctx, w);
     if (early) {
-        if (!ctx->check("route", launch_route_early(w, 4.0 * static_cast<double>(ctx->cell_budget),
+        if (!ctx->check("route", launch_route_early(w, 0.5 * static_cast<double>(ctx->cell_budget),
                                                     ctx->fs_route.ptr, max_points, ctx->sm_count, ctx->stream)))
             return false;
         FsWork es = w;

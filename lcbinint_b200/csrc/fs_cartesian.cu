@@ -793,7 +793,8 @@ __device__ __forceinline__ RowScratch rows_at(char* base, int cap, int seed_cap,
 }
 
 // The units of a split early point: seed ii's up scan is unit 2 ii, its down
-// scan unit 2 ii + 1, each with a SplitInfo and a kSplitRowCap-row scratch.
+// scan unit 2 ii + 1, each with a SplitInfo naming its kSplitRowCap-row
+// scratch area (slot) in the pool at `scratch`.
 struct SplitUse {
     const SplitInfo* info;
     char* scratch;
@@ -809,7 +810,7 @@ __device__ __forceinline__ SplitInfo load_info(const SplitInfo* p)
     v.yi_final = __ldcg(&p->yi_final);
     v.pred = __ldcg(&p->pred);
     v.ok = __ldcg(&p->ok);
-    v.pad = 0;
+    v.slot = __ldcg(&p->slot);
     for (int i = 0; i < 3; ++i) v.row0[i] = __ldcg(&p->row0[i]);
     return v;
 }
@@ -851,10 +852,10 @@ __device__ __noinline__ MergeOut merge_halves(RowScratch R, SplitUse sp, int ii,
     if (!U.ok || !D.ok) return m;
     const double inv_incr = 1.0 / incr;
     if (!(row_key(seed.y + (-incr), inv_incr) < row_key(seed.y, inv_incr))) return m;
-    const RowScratch UR = rows_at(sp.scratch + (long long)(2 * ii) * sp.bytes, kSplitRowCap, sp.seed_cap, nullptr,
+    const RowScratch UR = rows_at(sp.scratch + (long long)U.slot * sp.bytes, kSplitRowCap, sp.seed_cap, nullptr,
                                   nullptr);
-    const RowScratch DR = rows_at(sp.scratch + (long long)(2 * ii + 1) * sp.bytes, kSplitRowCap, sp.seed_cap,
-                                  nullptr, nullptr);
+    const RowScratch DR = rows_at(sp.scratch + (long long)D.slot * sp.bytes, kSplitRowCap, sp.seed_cap, nullptr,
+                                  nullptr);
     const int nu = U.yi_final;
     if (D.pred != (nu > 0 ? 1 : 0)) return m;
     const double x0m = __ldcg(UR.xmin), x0M = __ldcg(UR.xmax), y0 = __ldcg(UR.y);
@@ -1151,13 +1152,15 @@ __device__ void init_ctx(Ctx& C, const FsWork& w, const FsItem& item, const FsSe
 }
 
 // One unit of a split early point (early point e, seed ii, half 0 up or 1
-// down): the seed's directional scan at the point's source_bins into the
-// unit's own scratch, exactly as scan_point runs it (the down half first
-// scans the up scan's first row itself, for the bounds it starts from, and
-// counts only its own cells).  The result goes to the unit's SplitInfo; a
-// missing point or seed, or a scan that outgrows the unit's rows, leaves
-// ok = 0 and the finishing block scans that seed itself.
+// down): the seed's directional scan at the point's source_bins into a row
+// scratch area of its own, exactly as scan_point runs it (the down half
+// first scans the up scan's first row itself, for the bounds it starts
+// from, and counts only its own cells).  The result goes to the unit's
+// SplitInfo; a missing point or seed, a pool with no area left, or a scan
+// that outgrows the area's rows leaves ok = 0, and the finishing block scans
+// that seed itself.
 struct UnitArgs {
+    int* slots_taken;
     const int* early_cart;
     const int* ir_cart;
     const FsItem* items;
@@ -1182,7 +1185,17 @@ __device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e
     const int it = w.ir_cart[k];
     const FsItem item = w.items[it];
     const FsOut o = w.out[it];
+    int slot = -1;
     if (o.status == kFsOk && ii < o.n_seeds && item.rho > 0.0) {
+        if (Grp<W>::rank() == 0) {
+            const int a = atomicAdd(w.slots_taken, 1);
+            S.item = a < kSplitSlots ? a : -1;
+        }
+        Grp<W>::sync();
+        slot = S.item;
+        Grp<W>::sync();
+    }
+    if (slot >= 0) {
         const FsSettingsDev st = w.settings[item.settings];
         Ctx C;
         C.rays = 0;
@@ -1192,8 +1205,9 @@ __device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e
         lw.ld_tables = w.ld_tables;
         lw.f32_rays = w.f32_rays;
         init_ctx<W>(C, lw, item, st, nullptr, ld_smem, ld_loaded);
-        RowScratch R = rows_at(w.split_scratch + (long long)u * w.split_bytes, kSplitRowCap, w.seed_cap, nullptr,
+        RowScratch R = rows_at(w.split_scratch + (long long)slot * w.split_bytes, kSplitRowCap, w.seed_cap, nullptr,
                                nullptr);
+        info.slot = slot;
         R.gen = (epoch << 32) | 1ull;
         const double incr = item.rho / static_cast<double>(max(st.source_bins, 1));
         C.band = dmax_(4.0 * item.rho * incr, 4.0 * incr * incr);
@@ -1247,14 +1261,13 @@ __device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e
     return ld_loaded;
 }
 
-// Work items: the list's points in order, each with the scratch at `base`.
-// The early pass with split points (split_info set) takes first the units of
-// its first kSplitPoints points, kSplitSeeds seeds by two halves each, then
-// its other points; a point's scratch is the early pass's area at its list
-// position, and the block whose unit completes a split point's last unit
-// finishes that point from the units' rows (the units of a point run on
-// other blocks at the same time, so its scans take the time of the longest
-// half instead of the sum of all).
+// Work items: the list's points in order, each with the group's scratch at
+// `base`.  The early pass with split points (split_info set) takes instead
+// the units of its points, kSplitSeeds seeds by two halves each, in list
+// order (largest first), and the block whose unit completes a point's last
+// unit finishes that point from the units' rows: the units of a point run
+// on several blocks at once, so its scans take the time of the longest half
+// instead of the sum of all.
 template <int W>
 __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartList L, char* base, CartShared<W>& S,
                                TapeCell* tape, double* ld_smem = nullptr)
@@ -1268,7 +1281,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
     unsigned long long local_gen = 0;
     const int n = *L.count;
     const bool split = w.early_pass && w.split_info != nullptr && L.slots != nullptr;
-    const int n_split = split ? min(n, kSplitPoints) : 0;
+    const int n_split = split ? min(n, kEarlyMax) : 0;
     const int n_units = n_split * 2 * kSplitSeeds;
     const int n_work = split ? n_units + (n - n_split) : n;
     for (;;) {
@@ -1284,8 +1297,9 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         if (split) {
             if (idx < n_units) {
                 e = idx / (2 * kSplitSeeds);
-                const UnitArgs ua{w.early_cart, w.ir_cart, w.items, w.out, w.settings, w.ld_tables, w.seeds,
-                                  w.split_scratch, w.split_info, w.split_bytes, w.seed_cap, w.f32_rays};
+                const UnitArgs ua{w.ir_count + kSplitAlloc, w.early_cart, w.ir_cart, w.items, w.out, w.settings,
+                                  w.ld_tables, w.seeds, w.split_scratch, w.split_info, w.split_bytes, w.seed_cap,
+                                  w.f32_rays};
                 ld_loaded = run_unit<W>(ua, epoch, e, (idx >> 1) % kSplitSeeds, idx & 1, S, ld_smem, ld_loaded);
                 __threadfence();
                 Grp<W>::sync();
@@ -1293,20 +1307,15 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
                 Grp<W>::sync();
                 if (S.item != 2 * kSplitSeeds - 1) continue;
                 __threadfence();
-                su = SplitUse{w.split_info + (long long)e * 2 * kSplitSeeds,
-                              w.split_scratch + (long long)e * 2 * kSplitSeeds * w.split_bytes, w.split_bytes,
+                su = SplitUse{w.split_info + (long long)e * 2 * kSplitSeeds, w.split_scratch, w.split_bytes,
                               w.seed_cap};
                 use = &su;
             } else {
                 e = n_split + (idx - n_units);
             }
         }
-        if (w.early_pass) {
-            k = L.slots[e];
-            R = rows_at(w.scratch + (long long)e * w.scratch_per_warp, cap, w.seed_cap, &areaimage, &flags);
-        } else if (L.slots) {
-            k = L.slots[k];
-        }
+        if (w.early_pass) k = L.slots[e];
+        else if (L.slots) k = L.slots[k];
         if (W == 1 && !w.retry_pass && w.early_cart != nullptr) {
             // Points routed to the early block pass are not run here.
             const int ne = w.ir_count[5];
@@ -1436,9 +1445,7 @@ __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWo
     extern __shared__ double ld_smem[];
     const CartList L = w.early_pass ? CartList{w.early_cart, w.ir_count + 5, w.next_item + 6}
                                     : CartList{w.retry_cart, w.ir_count + 2, w.next_item + 3};
-    // The early pass takes its scratch by list position (cartesian_body).
-    char* base = w.early_pass ? w.scratch : w.scratch + (long long)blockIdx.x * w.scratch_per_warp;
-    cartesian_body<kBigWarps>(w, epoch, L, base, sh,
+    cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
                               w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr, ld_smem);
 }
 

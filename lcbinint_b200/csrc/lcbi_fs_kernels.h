@@ -138,18 +138,20 @@ struct FsWork {
     unsigned wait_limit;
     int* wait_timeouts;
     // Early points split into units (early pass only; split_info null: off):
-    // the up and the down scan of each of the first kSplitSeeds seeds of the
-    // first kSplitPoints early points run as separate work items, each on its
-    // own block and its own kSplitRowCap-row scratch (split_bytes each at
-    // split_scratch, unit u = (point * kSplitSeeds + seed) * 2 + half), and the
-    // block that completes a point's last unit (the point's counter at
+    // the up and the down scan of each of the first kSplitSeeds seeds of
+    // every early point run as separate work items, each on its own block
+    // (unit u = (point * kSplitSeeds + seed) * 2 + half, its SplitInfo at
+    // split_info[u]).  A unit that runs takes the next of kSplitSlots row
+    // scratch areas of kSplitRowCap rows (split_bytes each at split_scratch;
+    // ir_count[kSplitAlloc] counts the slots taken), and the block that
+    // completes a point's last unit (the point's counter at
     // ir_count[kSplitCounter + point]) finishes the point from their rows.
     char* split_scratch;
     long long split_bytes;
     struct SplitInfo* split_info;
 };
 
-constexpr int kEarlyMax = 32;
+constexpr int kEarlyMax = 512;
 
 // One unit of a split early point: what its half scan left.
 struct SplitInfo {
@@ -158,15 +160,21 @@ struct SplitInfo {
     int yi_final;             // the scan's row index when it returned
     int pred;                 // down half: index of the predecessor row (rows the first row's scan completed)
     int ok;                   // 1: the point, seed and scan exist and fit the unit's rows
-    int pad;
+    int slot;                 // its row scratch area
     double row0[3];           // down half: xmin, xmax and y of the first row of the up scan
 };
-constexpr int kSplitPoints = 16;
 constexpr int kSplitSeeds = 4;
-constexpr int kSplitUnits = kSplitPoints * kSplitSeeds * 2;
-constexpr int kSplitRowCap = 65536;
-constexpr int kSplitCounter = 64;  // ir_count[64, 64 + kSplitPoints): completed units per split point
-constexpr int kCounterInts = 128;  // size of the counters array (ir_count, next_item, early_cart, ...)
+constexpr int kSplitUnits = kEarlyMax * kSplitSeeds * 2;  // SplitInfo entries
+constexpr int kSplitSlots = 768;                           // unit row scratch areas
+constexpr int kSplitRowCap = 32768;
+// The counters array: ir_count [0, 8), next_item [8, 16), the route's
+// candidate count [48], the unit slots taken [kSplitAlloc], early_cart
+// [kEarlyOff, kEarlyOff + kEarlyMax), completed units per early point
+// [kSplitCounter, kSplitCounter + kEarlyMax).
+constexpr int kSplitAlloc = 49;
+constexpr int kEarlyOff = 64;
+constexpr int kSplitCounter = kEarlyOff + kEarlyMax;
+constexpr int kCounterInts = kSplitCounter + kEarlyMax;
 constexpr int kEarlyBlocks = 96;   // blocks of the early pass
 
 constexpr int kBigWarps = 8;

@@ -51,12 +51,12 @@ def _points(s, q, n, seed):
     return p[:, 0].copy(), p[:, 1].copy(), rho
 
 
-def _ring_points(rhos, n_other, seed):
+def _ring_points(rhos, n_other, seed, offset=1e-4):
     """Sources on the heavier lens of RING (Einstein rings, tens of thousands of
     lattice rows) followed by n_other sources around the lens."""
     rng = np.random.default_rng(seed)
     k = len(rhos)
-    y1 = np.concatenate([1e-4 + 1e-5 * np.arange(k), rng.uniform(-1.2, 1.2, n_other)])
+    y1 = np.concatenate([offset + 1e-5 * np.arange(k), rng.uniform(-1.2, 1.2, n_other)])
     y2 = np.concatenate([np.zeros(k), rng.uniform(-1.2, 1.2, n_other)])
     rho = np.concatenate([np.asarray(rhos, dtype=np.float64),
                           np.exp(rng.uniform(np.log(1e-3), np.log(3e-2), n_other))])
@@ -159,13 +159,13 @@ def test_noalloc_rings_past_the_fixed_limits_get_status_18_and_19():
     _lib_mod, L = _lib()
     ctx = _lib_mod.Context(0)
     try:
-        # Cartesian: a ring of rho = 2e-3 at 80 bins has about 85,000 rows in
-        # one seed's scans (the oracle's count), past 65,536; polar: rho = 1e-4
-        # at 20 bins has about 314,000 azimuthal rows of segments, past
-        # 262,144 slots.
-        for mode, rho_big, status in ((1, 2e-3, 18), (2, 1e-4, 19)):
+        # Cartesian: a ring of rho = 2e-3 at 80 bins (source 1e-4 from the
+        # lens) has about 85,000 rows in one seed's scans, past 65,536; polar:
+        # rho = 1e-4 at 20 bins with the source 5e-5 from the lens (a whole
+        # ring) visits about 272,000 segments, past 262,144 (the oracle's counts).
+        for mode, rho_big, offset, status in ((1, 2e-3, 1e-4, 18), (2, 1e-4, 5e-5, 19)):
             st = _settings(mode, 0.4, bins=80 if mode == 1 else 20)
-            y1, y2, rho = _ring_points([rho_big], 40, seed=mode)
+            y1, y2, rho = _ring_points([rho_big], 40, seed=mode, offset=offset)
             ref = _workspace(ctx, L, st, *RING, y1, y2, rho)
             assert ref["status"][0] == 0 and np.isfinite(ref["magnification"][0])
             got = _noalloc(ctx, L, st, *RING, y1, y2, rho)

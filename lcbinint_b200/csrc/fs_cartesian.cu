@@ -41,6 +41,8 @@ struct CartShared {
     unsigned cont[W];   // left scan: abscissa >= xmin(previous row) - dx
     int item;
     int red[W];
+    unsigned ev[W];     // gap-repair check: rows with a repair, per warp
+    double mx[W];       // and each warp's largest row jump
 };
 
 struct RowScratch {
@@ -1008,38 +1010,98 @@ __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* se
         };
         int nyi = yi;
         double areabound = 0.0;
-        for (int row = 0; row < nyi && !R.ovf; ++row) {
-            rows_ensure<W>(R, row + 1);
-            const double dxmax = R.xmax[row + 1] - R.xmax[row];
-            const double dxmin = R.xmin[row + 1] - R.xmin[row];
-            if (R.ax[row + 1] > 0.0) d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
-            if (R.ax[row + 1] > 0.0) {
-                if (dxmax > 1.1 * incr) {
-                    ++d.gap_repairs;
-                    table_ready();
-                    repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1],
-                              -R.dys[row], yi, js, areai, areabound);
+        // The repairs of one row (FSM:2576-2663), in the reference's order.
+        auto repair_row = [&](int row, double dxmax, double dxmin) {
+            if (dxmax > 1.1 * incr) {
+                ++d.gap_repairs;
+                table_ready();
+                repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1], -R.dys[row], yi,
+                          js, areai, areabound);
+            }
+            if (dxmin > 1.1 * incr) {
+                ++d.gap_repairs;
+                table_ready();
+                repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row], R.xmin[row + 1],
+                          R.dys[row], yi, js, areai, areabound);
+            }
+            if (dxmin < -1.1 * incr) {
+                ++d.gap_repairs;
+                table_ready();
+                repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row], -R.dys[row], yi,
+                          js, areai, areabound);
+            }
+            if (dxmax < -1.1 * incr) {
+                ++d.gap_repairs;
+                table_ready();
+                repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1], R.xmax[row],
+                          R.dys[row], yi, js, areai, areabound);
+            }
+        };
+        // The reference walks rows [0, nyi) one by one, and when its last row
+        // has added rows with area it walks those too.  A repair only writes
+        // rows from yi >= nyi on, so for every row but a walk's last one the
+        // row and its successor are as the scans left them: the group reads
+        // their conditions N rows at a time and runs the repairs they call
+        // for in row order.  The last row, whose successor a repair may have
+        // overwritten, is read after them, as the reference reads it.  The
+        // largest row jump is a maximum, so its order does not matter.
+        int lo = 0;
+        while (lo < nyi && !R.ovf) {
+            const int hi = nyi;
+            rows_ensure<W>(R, hi);
+            for (int base = lo; base < hi - 1 && !R.ovf; base += N) {
+                const int row = base + t;
+                bool ev = false;
+                double jmp = 0.0;
+                if (row < hi - 1 && R.ax[row + 1] > 0.0) {
+                    const double dxmax = R.xmax[row + 1] - R.xmax[row];
+                    const double dxmin = R.xmin[row + 1] - R.xmin[row];
+                    jmp = dmax_(fabs(dxmax), fabs(dxmin)) / incr;
+                    ev = dxmax > 1.1 * incr || dxmin > 1.1 * incr || dxmin < -1.1 * incr || dxmax < -1.1 * incr;
                 }
-                if (dxmin > 1.1 * incr) {
-                    ++d.gap_repairs;
-                    table_ready();
-                    repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row],
-                              R.xmin[row + 1], R.dys[row], yi, js, areai, areabound);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) jmp = dmax_(jmp, __shfl_xor_sync(kFull, jmp, o));
+                const unsigned wb = __ballot_sync(kFull, ev);
+                if (lane_id() == 0) {
+                    S.ev[Grp<W>::warp()] = wb;
+                    S.mx[Grp<W>::warp()] = jmp;
                 }
-                if (dxmin < -1.1 * incr) {
-                    ++d.gap_repairs;
-                    table_ready();
-                    repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row],
-                              -R.dys[row], yi, js, areai, areabound);
+                Grp<W>::sync();
+                unsigned evw[W];
+                double gm = 0.0;
+#pragma unroll
+                for (int w8 = 0; w8 < W; ++w8) {
+                    evw[w8] = S.ev[w8];
+                    gm = dmax_(gm, S.mx[w8]);
                 }
-                if (dxmax < -1.1 * incr) {
-                    ++d.gap_repairs;
-                    table_ready();
-                    repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1],
-                              R.xmax[row], R.dys[row], yi, js, areai, areabound);
+                Grp<W>::sync();
+                d.max_jump = dmax_(d.max_jump, gm);
+#pragma unroll 1
+                for (int w8 = 0; w8 < W && !R.ovf; ++w8) {
+                    unsigned m = evw[w8];
+                    while (m && !R.ovf) {
+                        const int r = base + 32 * w8 + __ffs(m) - 1;
+                        m &= m - 1u;
+                        repair_row(r, R.xmax[r + 1] - R.xmax[r], R.xmin[r + 1] - R.xmin[r]);
+                    }
                 }
             }
-            if (row == nyi - 1 && areabound > 0.0 && yi > nyi) nyi = yi;
+            if (!R.ovf) {
+                const int row = hi - 1;
+                rows_ensure<W>(R, row + 1);
+                const double dxmax = R.xmax[row + 1] - R.xmax[row];
+                const double dxmin = R.xmin[row + 1] - R.xmin[row];
+                if (R.ax[row + 1] > 0.0) {
+                    d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
+                    repair_row(row, dxmax, dxmin);
+                }
+            }
+            if (areabound > 0.0 && yi > nyi) {
+                lo = hi;
+                nyi = yi;
+            } else {
+                break;
+            }
         }
         if (R.ovf) {
             ovf = true;

@@ -1505,10 +1505,22 @@ __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWo
 {
     __shared__ CartShared<kBigWarps> sh;
     extern __shared__ double ld_smem[];
-    const CartList L = w.early_pass ? CartList{w.early_cart, w.ir_count + 5, w.next_item + 6}
-                                    : CartList{w.retry_cart, w.ir_count + 2, w.next_item + 3};
+    const CartList L{w.retry_cart, w.ir_count + 2, w.next_item + 3};
     cartesian_body<kBigWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh,
                               w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr, ld_smem);
+}
+
+// The early pass: blocks of kEarlyWarps warps, two per SM.  Its work is the
+// split points' seed-half units, each a serial row scan whose speed is set
+// by latency, not by the SM's issue rate, so two smaller groups per SM scan
+// about twice the rows of one large group in the same time.
+__global__ void __launch_bounds__(32 * kEarlyWarps, 2) cartesian_early_kernel(FsWork w, unsigned long long epoch)
+{
+    __shared__ CartShared<kEarlyWarps> sh;
+    extern __shared__ double ld_smem[];
+    const CartList L{w.early_cart, w.ir_count + 5, w.next_item + 6};
+    cartesian_body<kEarlyWarps>(w, epoch, L, w.scratch + (long long)blockIdx.x * w.scratch_per_warp, sh, nullptr,
+                                ld_smem);
 }
 
 } // namespace
@@ -1521,11 +1533,12 @@ size_t cartesian_scratch_bytes(int row_cap, int seed_cap)
 
 // First pass: one warp per point (n_groups warps).  Second pass
 // (w.retry_pass): one block of kBigWarps warps per point, n_groups blocks,
-// each with its own scratch.
+// each with its own scratch.  Early pass (w.early_pass): n_groups blocks of
+// kEarlyWarps warps, each with its own scratch.
 cudaError_t launch_cartesian(const FsWork& w, int n_groups, cudaStream_t stream, unsigned long long epoch)
 {
     if (w.retry_pass) {
-        // The shared-memory limit is a per-device attribute of the kernel, set
+        // The shared-memory limit is a per-device attribute of each kernel, set
         // before its first launch on each device (setting it again is harmless).
         static std::atomic<unsigned long long> attr_set{0};
         int dev = 0;
@@ -1535,10 +1548,16 @@ cudaError_t launch_cartesian(const FsWork& w, int n_groups, cudaStream_t stream,
         if (!(attr_set.load() & bit)) {
             e = cudaFuncSetAttribute(cartesian_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kBlockLdBytes));
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(cartesian_early_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kBlockLdBytes));
             if (e != cudaSuccess) return e;
             attr_set.fetch_or(bit);
         }
-        cartesian_block_kernel<<<n_groups, 32 * kBigWarps, kBlockLdBytes, stream>>>(w, epoch);
+        if (w.early_pass)
+            cartesian_early_kernel<<<n_groups, 32 * kEarlyWarps, kBlockLdBytes, stream>>>(w, epoch);
+        else
+            cartesian_block_kernel<<<n_groups, 32 * kBigWarps, kBlockLdBytes, stream>>>(w, epoch);
     } else {
         cartesian_warp_kernel<<<(n_groups + 3) / 4, 128, 0, stream>>>(w, epoch);
     }

@@ -175,7 +175,8 @@ constexpr int kSplitAlloc = 49;
 constexpr int kEarlyOff = 64;
 constexpr int kSplitCounter = kEarlyOff + kEarlyMax;
 constexpr int kCounterInts = kSplitCounter + kEarlyMax;
-constexpr int kEarlyBlocks = 96;   // blocks of the early pass
+constexpr int kEarlyWarps = 4;     // warps per block of the early pass (two blocks per SM)
+constexpr int kEarlyBlocks = 192;  // blocks of the early pass
 
 constexpr int kBigWarps = 8;
 

@@ -448,9 +448,11 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
             return false;
         ctx->stage_end(3, ev);
     }
-    ctx->stage_begin(3, &ev);
-    if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
-    ctx->stage_end(3, ev);
+    if (!overlap) {
+        ctx->stage_begin(3, &ev);
+        if (!ctx->check("cartesian", launch_cartesian(w, warps, ctx->stream, ctx->epoch))) return false;
+        ctx->stage_end(3, ev);
+    }
     FsWork r = w;
     r.retry_pass = 1;
     // The second pass's groups (blocks) have the tapes after the first pass's warps.
@@ -462,10 +464,10 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     r.row_cap = ctx->row_cap_big;
     r.queue_cap = ctx->queue_cap_big;
     r.hash_cap = ctx->hash_cap_big;
-    // The second Cartesian pass often holds one point for hundreds of
-    // milliseconds on one block.  Without stage timing it runs on the side
-    // stream, beside the polar passes, which would otherwise wait for it with
-    // the GPU nearly idle.  The two touch disjoint work lists, counters
+    // Without stage timing the Cartesian passes (the first on warps, then the
+    // second on blocks) run on the side stream, beside the polar passes, which
+    // need nothing from them: each alone leaves much of the GPU idle while its
+    // largest points finish.  The two touch disjoint work lists, counters
     // (Cartesian: ir_count[0], [2], next_item[1], [3]; polar: ir_count[1],
     // [3], next_item[2], [4]), outputs and scratch areas, so the results do
     // not depend on how they interleave.  With stage timing on, the stages run
@@ -474,8 +476,9 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         if (!ctx->check("fork", cudaEventRecord(ctx->fork_event, ctx->stream)) ||
             !ctx->check("fork", cudaStreamWaitEvent(ctx->side_stream, ctx->fork_event, 0)))
             return false;
-        const bool ok = ctx->check("cartesian retry",
-                                   launch_cartesian(r, retry_blocks(ctx), ctx->side_stream, ctx->epoch));
+        const bool ok =
+            ctx->check("cartesian", launch_cartesian(w, warps, ctx->side_stream, ctx->epoch)) &&
+            ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->side_stream, ctx->epoch));
         // The join is recorded even after a failed launch, so that the
         // context's stream never runs ahead of work already queued beside it.
         if (!ctx->check("join", cudaEventRecord(ctx->join_event, ctx->side_stream)) || !ok) return false;

@@ -176,7 +176,7 @@ constexpr int kEarlyOff = 64;
 constexpr int kSplitCounter = kEarlyOff + kEarlyMax;
 constexpr int kCounterInts = kSplitCounter + kEarlyMax;
 constexpr int kEarlyWarps = 4;     // warps per block of the early pass (two blocks per SM)
-constexpr int kEarlyBlocks = 192;  // blocks of the early pass
+constexpr int kEarlyBlocks = 96;   // blocks of the early pass
 
 constexpr int kBigWarps = 8;
 

@@ -2,6 +2,7 @@
 //   caustic models -> decision kernel -> seeding -> Cartesian / polar inverse ray.
 // The host only plans (de-duplicates lens models, builds constant angle tables
 // with the host C library) and launches; all physics runs in the kernels.
+#include <algorithm>
 #include "../../include/lcbinint_b200.h"
 #include "lcbi_context.h"
 #include "lcbi_fs_kernels.h"
@@ -95,14 +96,23 @@ size_t polar_bytes_big(const Context* c) { return (polar_scratch_bytes(c->queue_
 
 int retry_blocks(const Context* c) { return c->retry_blocks > 0 ? c->retry_blocks : c->sm_count; }
 
+// The early pass's blocks and unit row areas: kEarlyBlocks and kSplitSlots,
+// or, when the caller has set a number of second-pass blocks, as many early
+// blocks as second-pass blocks (at least 2) and 32 unit areas per early block.
+int early_blocks(const Context* c)
+{
+    return c->retry_blocks > 0 ? std::min(kEarlyBlocks, std::max(2, c->retry_blocks)) : kEarlyBlocks;
+}
+int split_slots(const Context* c) { return std::min(kSplitSlots, 32 * early_blocks(c)); }
+
 bool ensure_big_scratch(Context* ctx)
 {
     if (ctx->big_ready) return true;
     // Cartesian: the second pass's blocks, then the early pass's blocks.
-    const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + kEarlyBlocks);
+    const size_t cb = cart_bytes_big(ctx) * (retry_blocks(ctx) + early_blocks(ctx));
     const size_t pb = polar_bytes_big(ctx) * retry_blocks(ctx);
     // The units of the split early points: one small row scratch each.
-    const size_t sb = split_bytes(ctx) * kSplitSlots;
+    const size_t sb = split_bytes(ctx) * split_slots(ctx);
     if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb) ||
         !ctx->ensure(ctx->fs_split, sb) || !ctx->ensure(ctx->fs_split_info, kSplitUnits * sizeof(SplitInfo)))
         return false;
@@ -358,6 +368,7 @@ FsWork early_work(Context* ctx, const FsWork& w)
     e.split_scratch = static_cast<char*>(ctx->fs_split.ptr);
     e.split_bytes = static_cast<long long>(split_bytes(ctx));
     e.split_info = static_cast<SplitInfo*>(ctx->fs_split_info.ptr);
+    e.split_slots = split_slots(ctx);
     return e;
 }
 
@@ -399,7 +410,7 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
             const bool ok =
                 ctx->check("seeds early", launch_seeds(es, ctx->sm_count, ctx->early_stream, ek, ep, kEarlyMax)) &&
                 ctx->check("cartesian early",
-                           launch_cartesian(early_work(ctx, w), kEarlyBlocks, ctx->early_stream, ctx->epoch));
+                           launch_cartesian(early_work(ctx, w), early_blocks(ctx), ctx->early_stream, ctx->epoch));
             // Recorded even after a failed launch: the context's stream must
             // never run ahead of work already queued beside it.
             if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream))) return false;
@@ -444,7 +455,7 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
     if (ctx->early_serial) {
         // Stage timing on: the early block pass (stage_seeds) runs here, first.
         ctx->stage_begin(3, &ev);
-        if (!ctx->check("cartesian early", launch_cartesian(early_work(ctx, w), kEarlyBlocks, ctx->stream, ctx->epoch)))
+        if (!ctx->check("cartesian early", launch_cartesian(early_work(ctx, w), early_blocks(ctx), ctx->stream, ctx->epoch)))
             return false;
         ctx->stage_end(3, ev);
     }

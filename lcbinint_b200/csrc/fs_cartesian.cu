@@ -243,12 +243,13 @@ __device__ __forceinline__ double advance(double x0, double d, int t)
 
 // Evaluates the chunk of cells starting at ix along dx into shared memory:
 // cells [0, na).  With na < N the cells [na, N) hold a second segment, the
-// right scan (step -dx) of the row at sy from sx: the next row's first cells,
-// evaluated beside the current row's left scan (only left-scan fills carry
-// one).  na is a multiple of 32, so each warp evaluates one segment.
+// scan of the row at sy from sx in the other direction (step -dx): after a
+// left-scan chunk, the next row's first right-scan cells; after a row's first
+// right-scan chunk, its left-scan cells (whose continue bits use want_cont2
+// and thr2).  na is a multiple of 32, so each warp evaluates one segment.
 template <int W>
 __device__ void fill_chunk(Ctx& C, CartShared<W>& S, double ix, double iy, double dx, int jsign, bool want_cont,
-                           double thr, int na, double sx, double sy)
+                           double thr, int na, double sx, double sy, bool want_cont2 = false, double thr2 = 0.0)
 {
     const int t = Grp<W>::rank();
     Grp<W>::sync();  // every thread is done with the previous chunk
@@ -260,7 +261,7 @@ __device__ void fill_chunk(Ctx& C, CartShared<W>& S, double ix, double iy, doubl
     S.b[t] = b;
     S.x[t] = x;
     const unsigned in = __ballot_sync(kFull, d <= C.rho2);
-    const unsigned co = __ballot_sync(kFull, first && want_cont && x >= thr);
+    const unsigned co = __ballot_sync(kFull, first ? (want_cont && x >= thr) : (want_cont2 && x >= thr2));
     if (lane_id() == 0) {
         S.in[t >> 5] = in;
         S.cont[t >> 5] = co;
@@ -346,15 +347,23 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
     // (cur_xmax - incr) + incr, one row up or down, and cur_xmax no longer
     // changes once the row has a count.  The next row takes those cells when
     // its start matches bit for bit (spec_x, spec_y), so every cell the scan
-    // consumes has the value a fill at that position would give.
+    // consumes has the value a fill at that position would give.  Likewise a
+    // row's first right-scan fill (a scan's first row, a gap repair, or a
+    // row whose right end moved past the next-row cells) evaluates
+    // kFirstRight right-scan cells and, in chunk cells [kFirstRight, N), the
+    // row's left-scan cells from (x0 - incr), which the left scan takes when
+    // it starts there (lspec): a narrow row then needs one fill, not two.
     constexpr bool kSpec = W > 1;
     constexpr int kSpecCells = 32;
     constexpr int kSpecAt = N - kSpecCells;
+    constexpr int kFirstRight = 32;
     bool have = false;
     int cidx = 0, cend = N;
     double cdx = 0.0, cy = 0.0;
     bool spec = false;
     double spec_x = 0.0, spec_y = 0.0;
+    bool lspec = false, row_start = true;
+    double lspec_x = 0.0, lspec_y = 0.0;
     for (;;) {
         if (!(have && cidx < cend && cdx == dx && cy == iy)) {
             if (kSpec && spec && dx == incr && spec_x == ix && spec_y == iy) {
@@ -364,6 +373,13 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 cdx = dx;
                 cy = iy;
                 spec = false;
+            } else if (kSpec && lspec && dx == -incr && lspec_x == ix && lspec_y == iy) {
+                have = true;
+                cidx = kFirstRight;
+                cend = N;
+                cdx = dx;
+                cy = iy;
+                lspec = false;
             } else {
                 if (C.budget > 0 && C.evals > C.budget) {
                     R.ovf = true;  // hand the point to the second pass
@@ -371,18 +387,35 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
                 }
                 const bool want_cont = dx != incr && yi != 0;
                 const double thr = want_cont ? prev_xmin - dx : 0.0;
+                const bool first_right = kSpec && dx == incr && row_start;
                 const bool next_row = kSpec && dx != incr && countx != 0.0;
-                const double nx = next_row ? (cur_xmax - incr) + incr : 0.0;
-                const double ny = next_row ? iy + dy : 0.0;
-                fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr, next_row ? kSpecAt : N, nx, ny);
+                int na = N;
+                double nx = 0.0, ny = 0.0, thr2 = 0.0;
+                bool want_cont2 = false;
+                if (first_right) {
+                    na = kFirstRight;
+                    nx = x0 + (-incr);
+                    ny = iy;
+                    want_cont2 = yi != 0;
+                    thr2 = want_cont2 ? prev_xmin - (-incr) : 0.0;
+                } else if (next_row) {
+                    na = kSpecAt;
+                    nx = (cur_xmax - incr) + incr;
+                    ny = iy + dy;
+                }
+                fill_chunk<W>(C, S, ix, iy, dx, jsign, want_cont, thr, na, nx, ny, want_cont2, thr2);
                 have = true;
                 cidx = 0;
-                cend = next_row ? kSpecAt : N;
+                cend = na;
                 cdx = dx;
                 cy = iy;
                 spec = next_row;
                 spec_x = nx;
                 spec_y = ny;
+                lspec = first_right;
+                lspec_x = nx;
+                lspec_y = ny;
+                row_start = false;
             }
         }
         // Bulk step: consume the run of cells that only accumulate (inside cells of
@@ -510,6 +543,7 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
             key = row_key(iy, inv_incr);
             pre_h = key_hash(key, R.tmask);
             pre = R.table[pre_h];
+            row_start = true;
         }
         ix += dx;
     }
@@ -1223,6 +1257,7 @@ __device__ void init_ctx(Ctx& C, const FsWork& w, const FsItem& item, const FsSe
 // that seed itself.
 struct UnitArgs {
     int* slots_taken;
+    int split_slots;
     const int* early_cart;
     const int* ir_cart;
     const FsItem* items;
@@ -1251,7 +1286,7 @@ __device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e
     if (o.status == kFsOk && ii < o.n_seeds && item.rho > 0.0) {
         if (Grp<W>::rank() == 0) {
             const int a = atomicAdd(w.slots_taken, 1);
-            S.item = a < kSplitSlots ? a : -1;
+            S.item = a < w.split_slots ? a : -1;
         }
         Grp<W>::sync();
         slot = S.item;
@@ -1359,7 +1394,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         if (split) {
             if (idx < n_units) {
                 e = idx / (2 * kSplitSeeds);
-                const UnitArgs ua{w.ir_count + kSplitAlloc, w.early_cart, w.ir_cart, w.items, w.out, w.settings,
+                const UnitArgs ua{w.ir_count + kSplitAlloc, w.split_slots, w.early_cart, w.ir_cart, w.items, w.out, w.settings,
                                   w.ld_tables, w.seeds, w.split_scratch, w.split_info, w.split_bytes, w.seed_cap,
                                   w.f32_rays};
                 ld_loaded = run_unit<W>(ua, epoch, e, (idx >> 1) % kSplitSeeds, idx & 1, S, ld_smem, ld_loaded);

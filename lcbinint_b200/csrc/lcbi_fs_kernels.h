@@ -141,7 +141,7 @@ struct FsWork {
     // the up and the down scan of each of the first kSplitSeeds seeds of
     // every early point run as separate work items, each on its own block
     // (unit u = (point * kSplitSeeds + seed) * 2 + half, its SplitInfo at
-    // split_info[u]).  A unit that runs takes the next of kSplitSlots row
+    // split_info[u]).  A unit that runs takes the next of split_slots row
     // scratch areas of kSplitRowCap rows (split_bytes each at split_scratch;
     // ir_count[kSplitAlloc] counts the slots taken), and the block that
     // completes a point's last unit (the point's counter at
@@ -149,6 +149,7 @@ struct FsWork {
     char* split_scratch;
     long long split_bytes;
     struct SplitInfo* split_info;
+    int split_slots;   // row areas in the pool (at most kSplitSlots)
 };
 
 constexpr int kEarlyMax = 512;

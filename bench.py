@@ -934,7 +934,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=0,
-                    help="use only the first N points (small cases for profiler captures)")
+                    help="use only N points of the batch, chosen at random, with a small workspace (one "
+                         "first-pass warp per SM, eight second-pass blocks): small cases for profiler captures")
     ap.add_argument("--point", type=int, default=-1,
                     help="fs_batch: only point N of the batch, on a second-pass block (cell budget 1), with a "
                          "small workspace (one first-pass warp per SM, two second-pass blocks): the one-kernel "
@@ -1018,6 +1019,9 @@ def main():
     if args.point >= 0:
         ctx.check(L.lcbi_gpu_set_cell_budget(ctx.handle, 1), "lcbi_gpu_set_cell_budget")
         ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 2, 16384), "lcbi_gpu_set_workspace")
+    elif args.points > 0:
+        # A small case for profiler captures: about 2 GB of device workspace.
+        ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 8, 131072), "lcbi_gpu_set_workspace")
 
     settings, models, pts_all = fs_batch_arrays(rows)
     st_arr = (LcbiStructs.FsSettings * len(settings))(*settings)

@@ -339,31 +339,49 @@ __device__ __forceinline__ void quadratic(dc& x0, dc& x1, const dc* poly)
 
 } // namespace sg
 
+namespace sg {
+
+// newton_polish as one out-of-line copy: the solvers polish several roots
+// with the same code, and inlining it once per root made the point-source
+// kernel larger than the instruction cache (its largest stall was waiting
+// for instructions).  The polynomial goes by value, so no caller's
+// coefficients need an address.
+template <int N>
+__device__ __noinline__ dc polish_root(const PolyN<N> pn, dc root)
+{
+    newton_polish<N>(pn.c, root);
+    return root;
+}
+
+} // namespace sg
+
 // All five roots of the binary-lens quintic, cold start, polished.
 __device__ __forceinline__ void roots5(const dc* poly, dc* roots)
 {
     dc p2[6];
+    sg::PolyN<5> pn;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) p2[i] = poly[i];
+    for (int i = 0; i < 6; ++i) p2[i] = pn.c[i] = poly[i];
     roots[4] = sg::deflate_step<5>(p2);
     roots[3] = sg::deflate_step<4>(p2);
     roots[2] = sg::deflate_step<3>(p2);
     sg::quadratic(roots[1], roots[0], p2);
 #pragma unroll
-    for (int n = 0; n < 4; ++n) sg::newton_polish<5>(poly, roots[n]);
+    for (int n = 0; n < 4; ++n) roots[n] = sg::polish_root<5>(pn, roots[n]);
 }
 
 // All four roots of a quartic (critical-curve polynomial), cold start, polished.
 __device__ __forceinline__ void roots4(const dc* poly, dc* roots)
 {
     dc p2[5];
+    sg::PolyN<4> pn;
 #pragma unroll
-    for (int i = 0; i < 5; ++i) p2[i] = poly[i];
+    for (int i = 0; i < 5; ++i) p2[i] = pn.c[i] = poly[i];
     roots[3] = sg::deflate_step<4>(p2);
     roots[2] = sg::deflate_step<3>(p2);
     sg::quadratic(roots[1], roots[0], p2);
 #pragma unroll
-    for (int n = 0; n < 3; ++n) sg::newton_polish<4>(poly, roots[n]);
+    for (int n = 0; n < 3; ++n) roots[n] = sg::polish_root<4>(pn, roots[n]);
 }
 
 } // namespace lcbi

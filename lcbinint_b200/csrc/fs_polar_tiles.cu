@@ -134,23 +134,6 @@ __device__ void send_row(const TileCtx& G, int item, int tphi, int tr, int row, 
     if (atomicExch(&T->queued, 1) == 0) push_slot(G, (unsigned)s);
 }
 
-// Same for a whole warp: lane j ORs `bits` into row j (bits may be 0).
-__device__ void send_rows(const TileCtx& G, int item, int tphi, int tr, unsigned bits)
-{
-    long long s = -1;
-    if (lane_id() == 0) {
-        if (tr < (1 << kKeyBits) && tphi < (1 << kKeyBits)) s = find_or_insert(G, tile_key(item, tphi, tr));
-        if (s < 0) atomicExch(&G.items[item].state, kTileOverflow);
-    }
-    s = __shfl_sync(kFull, s, 0);
-    if (s < 0) return;
-    TileSlot* T = G.slots + s;
-    if (bits) atomicOr(&T->p[lane_id()], bits);
-    __threadfence();
-    __syncwarp();
-    if (lane_id() == 0 && atomicExch(&T->queued, 1) == 0) push_slot(G, (unsigned)s);
-}
-
 // Cells reachable from g by moving up, then down, through set bits of p
 // (Kogge-Stone occluded fills; g must be a subset of p).
 __device__ __forceinline__ unsigned fill_row(unsigned g, unsigned p)
@@ -198,16 +181,24 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
 {
     const int j = lane_id();
     TileSlot* T = G.slots + slot;
-    const unsigned long long key = ld_cg_u64(&T->key) - 1ull;
-    const int item = static_cast<int>(key >> (2 * kKeyBits));
-    const int tphi = static_cast<int>((key >> kKeyBits) & kKeyMask);
-    const int tr = static_cast<int>(key & kKeyMask);
-    const TileItem I = G.items[item];
+    // The queued flag is cleared before the pending bits are taken (a sender
+    // ORs its bits, then sets the flag), so bits that arrive after the take
+    // queue the tile again.  The key, the item and the mask flag do not
+    // depend on either and are read meanwhile, so a visit starts after about
+    // three L2 round trips instead of six.
     if (j == 0) atomicExch(&T->queued, 0);
+    const unsigned long long key = ld_cg_u64(&T->key) - 1ull;
     __syncwarp();
     __threadfence();
     const unsigned pend = atomicExch(&T->p[j], 0u);
-    if (ld_cg_i32(&G.items[item].state) != kTileActive) return;
+    int ready = 0;
+    if (j == 0) ready = ld_cg_i32(&T->mready);
+    const int item = static_cast<int>(key >> (2 * kKeyBits));
+    const int tphi = static_cast<int>((key >> kKeyBits) & kKeyMask);
+    const int tr = static_cast<int>(key & kKeyMask);
+    const int state = ld_cg_i32(&G.items[item].state);
+    const TileItem I = G.items[item];
+    if (state != kTileActive) return;
     const int g = tphi * 32 + j;
     const bool valid = g < I.phi_bins;
     double cs = 0.0, sn = 0.0;
@@ -221,8 +212,6 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
         const double ra = (static_cast<double>(tr * 32) + 16.0) * I.dr;
         A = make_anchor32(I.m, ra * cs, ra * sn, I.src);
     }
-    int ready = 0;
-    if (j == 0) ready = ld_cg_i32(&T->mready);
     ready = __shfl_sync(kFull, ready, 0);
     unsigned M = 0;
     const bool fresh = ready == 0;
@@ -290,22 +279,40 @@ __device__ void process_tile(const TileCtx& G, unsigned slot, double* d2s)
         atomicAdd(reinterpret_cast<unsigned long long*>(&Ig->acc_hi), (unsigned long long)(acc.hi + carry));
         atomicAdd(&Ig->cells, (unsigned long long)cnt);
     }
-    // Exits along r.
-    if (__any_sync(kFull, (nw >> 31) != 0u)) send_rows(G, item, tphi, tr + 1, (nw >> 31) ? 1u : 0u);
-    if (tr > 0 && __any_sync(kFull, (nw & 1u) != 0u)) send_rows(G, item, tphi, tr - 1, (nw & 1u) ? 0x80000000u : 0u);
-    // Exits along phi (periodic): the tile's last row (or the lattice's last
-    // row) upwards, its first row downwards.
-    if (valid && nw) {
-        const int P = I.phi_bins;
-        if (j == 31 || g == P - 1) {
-            const int gu = (g + 1 == P) ? 0 : g + 1;
-            send_row(G, item, gu >> 5, tr, gu & 31, nw);
-        }
-        if (j == 0) {
-            const int gd = (g == 0) ? P - 1 : g - 1;
-            send_row(G, item, gd >> 5, tr, gd & 31, nw);
+    // Exits, at most four neighbour tiles: along r outwards (the rows' last
+    // cells) and inwards (their first cells), along phi upwards from the
+    // tile's last row (or the lattice's last row; phi is periodic) and
+    // downwards from its first row.  Lane k of lanes 0-3 looks up exit k's
+    // tile, every lane ORs its bits into the r exits' rows, lanes 2 and 3
+    // into the phi exits' rows, and lane k queues tile k: the four exits
+    // cost the round trips of one.
+    const int P = I.phi_bins;
+    const int ju = (tphi * 32 + 31 < P) ? 31 : P - 1 - tphi * 32;  // the lattice row below the upward exit
+    const unsigned nw_up = __shfl_sync(kFull, valid ? nw : 0u, ju);
+    const unsigned nw_dn = __shfl_sync(kFull, valid ? nw : 0u, 0);
+    const bool out_r = __any_sync(kFull, (nw >> 31) != 0u);
+    const bool in_r = tr > 0 && __any_sync(kFull, (nw & 1u) != 0u);
+    const int g_up = tphi * 32 + ju, g_dn = tphi * 32;
+    const int gu = (g_up + 1 == P) ? 0 : g_up + 1;
+    const int gd = (g_dn == 0) ? P - 1 : g_dn - 1;
+    long long s_mine = -1;
+    if (j < 4) {
+        const bool active = j == 0 ? out_r : (j == 1 ? in_r : (j == 2 ? nw_up != 0u : nw_dn != 0u));
+        const int xr = j == 0 ? tr + 1 : (j == 1 ? tr - 1 : tr);
+        const int xphi = j < 2 ? tphi : (j == 2 ? gu >> 5 : gd >> 5);
+        if (active) {
+            if (xr < (1 << kKeyBits) && xphi < (1 << kKeyBits)) s_mine = find_or_insert(G, tile_key(item, xphi, xr));
+            if (s_mine < 0) atomicExch(&G.items[item].state, kTileOverflow);
         }
     }
+    const long long s0 = __shfl_sync(kFull, s_mine, 0), s1 = __shfl_sync(kFull, s_mine, 1);
+    if (s0 >= 0 && (nw >> 31)) atomicOr(&G.slots[s0].p[j], 1u);
+    if (s1 >= 0 && (nw & 1u)) atomicOr(&G.slots[s1].p[j], 0x80000000u);
+    if (j == 2 && s_mine >= 0) atomicOr(&G.slots[s_mine].p[gu & 31], nw_up);
+    if (j == 3 && s_mine >= 0) atomicOr(&G.slots[s_mine].p[gd & 31], nw_dn);
+    __threadfence();
+    __syncwarp();
+    if (s_mine >= 0 && atomicExch(&G.slots[s_mine].queued, 1) == 0) push_slot(G, (unsigned)s_mine);
 }
 
 // Persistent warps.  A warp takes a ticket (one atomicAdd on the FIFO head, so

@@ -40,6 +40,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "finite-source mags/s & rays/s on 1 B200 at 1e-4 rel err; fwd+grad/fwd ratio"
 F_RAY = 32.0      # algorithmic flop per lens-map evaluation of one cell
+# DRAM traffic measured with ncu (small single-kernel captures): the early
+# Cartesian scan of the batch's largest point read 4.22 MB and wrote nothing
+# for its 6.35e6 counted cells; the point-source kernel moved 32.17 MB per
+# 1e6 positions.  The scans generate their lattice on the fly, so their
+# traffic is a few bytes per thousand flop: HBM is not their bound.
+RAY_DRAM_BYTES_PER_CELL = 4.222464e6 / 6.349603e6
+PS_DRAM_BYTES = 32.158976e6 + 7.68e3
 F_PS = 3500.0     # algorithmic FP64 flop per point-source solve
 
 # --------------------------------------------------------------------------- workloads
@@ -641,7 +648,10 @@ def run_other_workload(args, world, rank, local_rank, ncores):
                            "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
                            "peak_no_fma": peak.value / 2.0,
                            "frac_of_no_fma_peak": 2.0 * achieved / peak.value if peak.value else None,
-                           "traffic": None, "flop_per_solve": F_PS,
+                           "traffic": PS_DRAM_BYTES * n / 1e6,
+                           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 1e6-point "
+                                             "launch, scaled by points",
+                           "flop_per_solve": F_PS,
                            "peak_source": "device-measured FP64 FMA loop (lcbi_gpu_measure_fp64_peak); the no-FMA "
                                           "figure is half of it (the kernel is built without contraction)"}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
@@ -1163,7 +1173,9 @@ def main():
                 "frac": achieved / chip_peak if chip_peak else None,
                 "peak_no_fma": chip_peak / 2.0,
                 "frac_of_no_fma_peak": 2.0 * achieved / chip_peak if chip_peak else None,
-                "traffic": None,
+                "traffic": RAY_DRAM_BYTES_PER_CELL * rays_all,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the early-pass scan of "
+                                  "point 1285 (6.35e6 cells), per cell, times the step's counted cells",
                 "peak_source": "device-measured FP64 FMA loop (lcbi_gpu_measure_fp64_peak) x GPUs; the no-FMA "
                                "figure is half of it (one flop per FP64 instruction)",
                 "achieved_over": "ms_per_step (device-timed steps): counted cells of the step x flop_per_ray",

@@ -948,7 +948,8 @@ def main():
                          "first-pass warp per SM, eight second-pass blocks): small cases for profiler captures")
     ap.add_argument("--point", type=int, default=-1,
                     help="fs_batch: only point N of the batch, on a second-pass block (cell budget 1), with a "
-                         "small workspace (one first-pass warp per SM, two second-pass blocks): the one-kernel "
+                         "small workspace (one first-pass warp per SM, eight second-pass blocks, hence eight "
+                         "early-pass blocks for its seed-half units): the one-kernel "
                          "case for profiler captures of the block scan (point 1285: the batch's largest "
                          "Cartesian point)")
     ap.add_argument("--rays", default="f64", choices=["f64", "f32"],
@@ -1028,7 +1029,7 @@ def main():
     L.lcbi_gpu_set_stream(ctx.handle, stream.cuda_stream)
     if args.point >= 0:
         ctx.check(L.lcbi_gpu_set_cell_budget(ctx.handle, 1), "lcbi_gpu_set_cell_budget")
-        ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 2, 16384), "lcbi_gpu_set_workspace")
+        ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 8, 16384), "lcbi_gpu_set_workspace")
     elif args.points > 0:
         # A small case for profiler captures: about 2 GB of device workspace.
         ctx.check(L.lcbi_gpu_set_workspace(ctx.handle, 1, 8, 131072), "lcbi_gpu_set_workspace")

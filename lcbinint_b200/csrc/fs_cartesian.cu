@@ -323,7 +323,7 @@ __device__ __forceinline__ double chunk_sum(CartShared<W>& S, double acc, int a,
 // overlaps the row's lens-map evaluations.
 template <int W>
 __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, double dy, int& yi, int jsign,
-                             int stop_rows = 0)
+                             int stop_rows = 0, bool have_pred = false, double pred_xmin = 0.0)
 {
     constexpr int N = Grp<W>::N;
     double countx = 0.0, countall = 0.0, dz2 = 99999999.9;
@@ -340,7 +340,9 @@ __device__ double image_area(Ctx& C, RowScratch& R, CartShared<W>& S, P2 seed, d
     double prev_xmin = 0.0, cur_xmin = 0.0, cur_xmax = 0.0;
     rows_ensure<W>(R, yi);
     if (R.ovf) return countall;
-    if (yi > 0) prev_xmin = R.xmin[yi - 1];
+    // The predecessor row's xmin: given by a caller that has just written it
+    // (a gap repair), which saves reading it back.
+    if (yi > 0) prev_xmin = have_pred ? pred_xmin : R.xmin[yi - 1];
     // Row-key table slot of the current row, fetched ahead.
     int key = row_key(iy, inv_incr);
     unsigned pre_h = key_hash(key, R.tmask);
@@ -613,9 +615,10 @@ __device__ __forceinline__ void repair(Ctx& C, RowScratch& R, CartShared<W>& S, 
     wset<W>(R.xmin, yi, xmin_v);
     wset<W>(R.xmax, yi, xmax_v);
     wset<W>(R.dys, yi, dy);
-    Grp<W>::sync();
+    // The scan reads no field of the predecessor row but its xmin, which it
+    // is given; the barrier after the scan publishes rank 0's writes.
     ++yi;
-    const double area0 = image_area<W>(C, R, S, es, dy, yi, js);
+    const double area0 = image_area<W>(C, R, S, es, dy, yi, js, 0, true, xmin_v);
     Grp<W>::sync();  // rows written by rank 0 just before the scan ended
     areai += area0;
     areabound += area0;

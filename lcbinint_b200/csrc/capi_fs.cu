@@ -114,7 +114,8 @@ bool ensure_big_scratch(Context* ctx)
     // The units of the split early points: one small row scratch each.
     const size_t sb = split_bytes(ctx) * split_slots(ctx);
     if (!ctx->ensure(ctx->fs_scratch_big, cb) || !ctx->ensure(ctx->fs_scratch_polar_big, pb) ||
-        !ctx->ensure(ctx->fs_split, sb) || !ctx->ensure(ctx->fs_split_info, kSplitUnits * sizeof(SplitInfo)))
+        !ctx->ensure(ctx->fs_split, sb) || !ctx->ensure(ctx->fs_split_info, kSplitUnits * sizeof(SplitInfo)) ||
+        !ctx->ensure(ctx->fs_seed_info, (size_t)kEarlyMax * kSplitSeeds * sizeof(SeedInfo)))
         return false;
     if (!ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_big.ptr, 0xff, cb, ctx->stream)) ||
         !ctx->check("scratch init", cudaMemsetAsync(ctx->fs_scratch_polar_big.ptr, 0xff, pb, ctx->stream)) ||
@@ -369,6 +370,7 @@ FsWork early_work(Context* ctx, const FsWork& w)
     e.split_bytes = static_cast<long long>(split_bytes(ctx));
     e.split_info = static_cast<SplitInfo*>(ctx->fs_split_info.ptr);
     e.split_slots = split_slots(ctx);
+    e.seed_info = static_cast<SeedInfo*>(ctx->fs_seed_info.ptr);
     return e;
 }
 

@@ -844,6 +844,7 @@ struct SplitUse {
     char* scratch;
     long long bytes;
     int seed_cap;
+    const SeedInfo* seeds;  // the point's seeds after their gap repairs (kSplitSeeds)
 };
 
 __device__ __forceinline__ SplitInfo load_info(const SplitInfo* p)
@@ -964,6 +965,162 @@ __device__ __noinline__ bool fill_table(RowScratch R, int n_up, int yi, double i
     return Grp<W>::any(full);
 }
 
+// A seed whose split units and gap repairs are done: its rows [0, nyi]
+// copied from the up half's area into R, and its results.  ok = false (R
+// untouched) when the seed's block could not complete it.
+struct SeedTake {
+    bool ok;
+    int nyi, repairs;
+    double areai, max_jump;
+    unsigned long long rays;
+};
+
+template <int W>
+__device__ __noinline__ SeedTake take_seed(RowScratch R, SplitUse sp, int ii)
+{
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
+    SeedTake k{false, 0, 0, 0.0, 0.0, 0ull};
+    const SeedInfo* p = sp.seeds + ii;
+    if (__ldcg(&p->ok) != 1) return k;
+    const int nyi = __ldcg(&p->nyi);
+    if (nyi + 1 > R.cap) return k;
+    const RowScratch UR = rows_at(sp.scratch + (long long)__ldcg(&sp.info[2 * ii].slot) * sp.bytes, kSplitRowCap,
+                                  sp.seed_cap, nullptr, nullptr);
+    for (int r = t; r <= nyi; r += N) {
+        R.xmin[r] = __ldcg(UR.xmin + r);
+        R.xmax[r] = __ldcg(UR.xmax + r);
+        R.ax[r] = __ldcg(UR.ax + r);
+        R.y[r] = __ldcg(UR.y + r);
+        R.dys[r] = __ldcg(UR.dys + r);
+    }
+    Grp<W>::sync();
+    k.ok = true;
+    k.nyi = nyi;
+    k.repairs = __ldcg(&p->repairs);
+    k.areai = __ldcg(&p->areai);
+    k.max_jump = __ldcg(&p->max_jump);
+    k.rays = __ldcg(&p->rays);
+    return k;
+}
+
+// The gap-repair walk of one seed's rows (FSM:2576-2663, the rows loop of
+// inverse_ray_cartesian_binary_mag) after its two directional scans, which
+// left yi rows and the area areai; n_up >= 0: the scans came from split units
+// and their rows enter the row-key table before the first repair.  Returns
+// the walk's final row count nyi (the rows the bookkeeping reads); the
+// largest row jump and the repair count accumulate into max_jump and
+// gap_repairs.
+template <int W>
+__device__ __forceinline__ int repair_walk(Ctx& C, RowScratch& R, CartShared<W>& S, int js, double incr, int& yi,
+                                           double& areai, int n_up, double& max_jump, int& gap_repairs)
+{
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
+    auto table_ready = [&]() {
+        if (n_up >= 0) {
+            if (fill_table<W>(R, n_up, yi, incr)) R.ovf = true;
+            n_up = -1;
+        }
+    };
+    int nyi = yi;
+    double areabound = 0.0;
+    // The repairs of one row (FSM:2576-2663), in the reference's order.
+    auto repair_row = [&](int row, double dxmax, double dxmin) {
+        if (dxmax > 1.1 * incr) {
+            ++gap_repairs;
+            table_ready();
+            repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1], -R.dys[row], yi,
+                      js, areai, areabound);
+        }
+        if (dxmin > 1.1 * incr) {
+            ++gap_repairs;
+            table_ready();
+            repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row], R.xmin[row + 1],
+                      R.dys[row], yi, js, areai, areabound);
+        }
+        if (dxmin < -1.1 * incr) {
+            ++gap_repairs;
+            table_ready();
+            repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row], -R.dys[row], yi,
+                      js, areai, areabound);
+        }
+        if (dxmax < -1.1 * incr) {
+            ++gap_repairs;
+            table_ready();
+            repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1], R.xmax[row],
+                      R.dys[row], yi, js, areai, areabound);
+        }
+    };
+    // The reference walks rows [0, nyi) one by one, and when its last row
+    // has added rows with area it walks those too.  A repair only writes
+    // rows from yi >= nyi on, so for every row but a walk's last one the
+    // row and its successor are as the scans left them: the group reads
+    // their conditions N rows at a time and runs the repairs they call
+    // for in row order.  The last row, whose successor a repair may have
+    // overwritten, is read after them, as the reference reads it.  The
+    // largest row jump is a maximum, so its order does not matter.
+    int lo = 0;
+    while (lo < nyi && !R.ovf) {
+        const int hi = nyi;
+        rows_ensure<W>(R, hi);
+        for (int base = lo; base < hi - 1 && !R.ovf; base += N) {
+            const int row = base + t;
+            bool ev = false;
+            double jmp = 0.0;
+            if (row < hi - 1 && R.ax[row + 1] > 0.0) {
+                const double dxmax = R.xmax[row + 1] - R.xmax[row];
+                const double dxmin = R.xmin[row + 1] - R.xmin[row];
+                jmp = dmax_(fabs(dxmax), fabs(dxmin)) / incr;
+                ev = dxmax > 1.1 * incr || dxmin > 1.1 * incr || dxmin < -1.1 * incr || dxmax < -1.1 * incr;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) jmp = dmax_(jmp, __shfl_xor_sync(kFull, jmp, o));
+            const unsigned wb = __ballot_sync(kFull, ev);
+            if (lane_id() == 0) {
+                S.ev[Grp<W>::warp()] = wb;
+                S.mx[Grp<W>::warp()] = jmp;
+            }
+            Grp<W>::sync();
+            unsigned evw[W];
+            double gm = 0.0;
+#pragma unroll
+            for (int w8 = 0; w8 < W; ++w8) {
+                evw[w8] = S.ev[w8];
+                gm = dmax_(gm, S.mx[w8]);
+            }
+            Grp<W>::sync();
+            max_jump = dmax_(max_jump, gm);
+#pragma unroll 1
+            for (int w8 = 0; w8 < W && !R.ovf; ++w8) {
+                unsigned m = evw[w8];
+                while (m && !R.ovf) {
+                    const int r = base + 32 * w8 + __ffs(m) - 1;
+                    m &= m - 1u;
+                    repair_row(r, R.xmax[r + 1] - R.xmax[r], R.xmin[r + 1] - R.xmin[r]);
+                }
+            }
+        }
+        if (!R.ovf) {
+            const int row = hi - 1;
+            rows_ensure<W>(R, row + 1);
+            const double dxmax = R.xmax[row + 1] - R.xmax[row];
+            const double dxmin = R.xmin[row + 1] - R.xmin[row];
+            if (R.ax[row + 1] > 0.0) {
+                max_jump = dmax_(max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
+                repair_row(row, dxmax, dxmin);
+            }
+        }
+        if (areabound > 0.0 && yi > nyi) {
+            lo = hi;
+            nyi = yi;
+        } else {
+            break;
+        }
+    }
+    return nyi;
+}
+
 // One scan of a point's lattice (inverse_ray_cartesian_binary_mag,
 // FSM:2470-2768) at `source_bins` cells per source radius: the directional
 // flood fills of every seed that no earlier seed's rows cover, their gap
@@ -1007,17 +1164,20 @@ __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* se
         const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
         ++d.processed;
         if (js != 0) ++d.fold;
-        // n_up >= 0: the two scans came from the seed's split units, and their
-        // rows enter the row-key table before the first gap repair.
-        int n_up = -1;
-        MergeOut mo{false, 0, 0, 0, 0.0, 0ull};
-        if (sp != nullptr && ii < kSplitSeeds) mo = merge_halves<W>(R, *sp, ii, seed, incr);
-        if (mo.ok) {
-            yi = mo.yi;
-            n_up = mo.n_up;
-            R.hw = mo.hw;
-            areai = mo.areai;
-            C.rays += mo.rays;
+        // A split point's first kSplitSeeds seeds come scanned and repaired
+        // from their units (seed_finish); the others, and any seed its
+        // block could not complete, are scanned here.
+        int nyi = 0;
+        SeedTake tk{false, 0, 0, 0.0, 0.0, 0ull};
+        if (sp != nullptr && ii < kSplitSeeds) tk = take_seed<W>(R, *sp, ii);
+        if (tk.ok) {
+            nyi = tk.nyi;
+            yi = tk.nyi;
+            R.hw = tk.nyi + 1;
+            areai = tk.areai;
+            C.rays += tk.rays;
+            d.max_jump = dmax_(d.max_jump, tk.max_jump);
+            d.gap_repairs += tk.repairs;
         } else {
             wset<W>(R.xmin, 0, seed.x);
             wset<W>(R.xmax, 0, seed.x);
@@ -1043,107 +1203,7 @@ __device__ bool scan_point(Ctx& C, RowScratch& R, CartShared<W>& S, const P2* se
             ++yi;
             areai += image_area<W>(C, R, S, lower, dy, yi, js);
             Grp<W>::sync();
-        }
-        auto table_ready = [&]() {
-            if (n_up >= 0) {
-                if (fill_table<W>(R, n_up, yi, incr)) R.ovf = true;
-                n_up = -1;
-            }
-        };
-        int nyi = yi;
-        double areabound = 0.0;
-        // The repairs of one row (FSM:2576-2663), in the reference's order.
-        auto repair_row = [&](int row, double dxmax, double dxmin) {
-            if (dxmax > 1.1 * incr) {
-                ++d.gap_repairs;
-                table_ready();
-                repair<W>(C, R, S, P2{R.xmax[row + 1], R.y[row]}, R.xmax[row], R.xmax[row + 1], -R.dys[row], yi,
-                          js, areai, areabound);
-            }
-            if (dxmin > 1.1 * incr) {
-                ++d.gap_repairs;
-                table_ready();
-                repair<W>(C, R, S, P2{R.xmin[row + 1] - incr, R.y[row + 1]}, R.xmin[row], R.xmin[row + 1],
-                          R.dys[row], yi, js, areai, areabound);
-            }
-            if (dxmin < -1.1 * incr) {
-                ++d.gap_repairs;
-                table_ready();
-                repair<W>(C, R, S, P2{R.xmin[row] - incr, R.y[row]}, R.xmin[row + 1], R.xmin[row], -R.dys[row], yi,
-                          js, areai, areabound);
-            }
-            if (dxmax < -1.1 * incr) {
-                ++d.gap_repairs;
-                table_ready();
-                repair<W>(C, R, S, P2{R.xmax[row + 1] + incr, R.y[row + 1]}, R.xmax[row + 1], R.xmax[row],
-                          R.dys[row], yi, js, areai, areabound);
-            }
-        };
-        // The reference walks rows [0, nyi) one by one, and when its last row
-        // has added rows with area it walks those too.  A repair only writes
-        // rows from yi >= nyi on, so for every row but a walk's last one the
-        // row and its successor are as the scans left them: the group reads
-        // their conditions N rows at a time and runs the repairs they call
-        // for in row order.  The last row, whose successor a repair may have
-        // overwritten, is read after them, as the reference reads it.  The
-        // largest row jump is a maximum, so its order does not matter.
-        int lo = 0;
-        while (lo < nyi && !R.ovf) {
-            const int hi = nyi;
-            rows_ensure<W>(R, hi);
-            for (int base = lo; base < hi - 1 && !R.ovf; base += N) {
-                const int row = base + t;
-                bool ev = false;
-                double jmp = 0.0;
-                if (row < hi - 1 && R.ax[row + 1] > 0.0) {
-                    const double dxmax = R.xmax[row + 1] - R.xmax[row];
-                    const double dxmin = R.xmin[row + 1] - R.xmin[row];
-                    jmp = dmax_(fabs(dxmax), fabs(dxmin)) / incr;
-                    ev = dxmax > 1.1 * incr || dxmin > 1.1 * incr || dxmin < -1.1 * incr || dxmax < -1.1 * incr;
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) jmp = dmax_(jmp, __shfl_xor_sync(kFull, jmp, o));
-                const unsigned wb = __ballot_sync(kFull, ev);
-                if (lane_id() == 0) {
-                    S.ev[Grp<W>::warp()] = wb;
-                    S.mx[Grp<W>::warp()] = jmp;
-                }
-                Grp<W>::sync();
-                unsigned evw[W];
-                double gm = 0.0;
-#pragma unroll
-                for (int w8 = 0; w8 < W; ++w8) {
-                    evw[w8] = S.ev[w8];
-                    gm = dmax_(gm, S.mx[w8]);
-                }
-                Grp<W>::sync();
-                d.max_jump = dmax_(d.max_jump, gm);
-#pragma unroll 1
-                for (int w8 = 0; w8 < W && !R.ovf; ++w8) {
-                    unsigned m = evw[w8];
-                    while (m && !R.ovf) {
-                        const int r = base + 32 * w8 + __ffs(m) - 1;
-                        m &= m - 1u;
-                        repair_row(r, R.xmax[r + 1] - R.xmax[r], R.xmin[r + 1] - R.xmin[r]);
-                    }
-                }
-            }
-            if (!R.ovf) {
-                const int row = hi - 1;
-                rows_ensure<W>(R, row + 1);
-                const double dxmax = R.xmax[row + 1] - R.xmax[row];
-                const double dxmin = R.xmin[row + 1] - R.xmin[row];
-                if (R.ax[row + 1] > 0.0) {
-                    d.max_jump = dmax_(d.max_jump, dmax_(fabs(dxmax), fabs(dxmin)) / incr);
-                    repair_row(row, dxmax, dxmin);
-                }
-            }
-            if (areabound > 0.0 && yi > nyi) {
-                lo = hi;
-                nyi = yi;
-            } else {
-                break;
-            }
+            nyi = repair_walk<W>(C, R, S, js, incr, yi, areai, -1, d.max_jump, d.gap_repairs);
         }
         if (R.ovf) {
             ovf = true;
@@ -1266,6 +1326,7 @@ __device__ void init_ctx(Ctx& C, const FsWork& w, const FsItem& item, const FsSe
 struct UnitArgs {
     int* slots_taken;
     int split_slots;
+    SeedInfo* seed_info;
     const int* early_cart;
     const int* ir_cart;
     const FsItem* items;
@@ -1366,6 +1427,84 @@ __device__ __noinline__ int run_unit(UnitArgs w, unsigned long long epoch, int e
     return ld_loaded;
 }
 
+// The second block to complete one of seed ii's halves (early point e)
+// finishes the seed: it merges the two halves in its own scratch R, runs the
+// seed's gap repairs there (a seed's rows and repairs touch no other seed's),
+// and leaves the rows [0, nyi] in the up half's area and the results in the
+// seed's SeedInfo, for the block that finishes the point.  A missing seed, a
+// merge that cannot be taken, an overflow, or rows past the area leave
+// ok = 0 and that block scans the seed itself.  The row-key tags use the
+// epoch with a per-seed generation above every generation of scan_point.
+template <int W>
+__device__ __noinline__ int seed_finish(UnitArgs w, unsigned long long epoch, int e, int ii, CartShared<W>& S,
+                                        double* ld_smem, int ld_loaded, RowScratch R)
+{
+    constexpr int N = Grp<W>::N;
+    const int t = Grp<W>::rank();
+    SeedInfo out{};
+    const int k = w.early_cart[e];
+    const int it = w.ir_cart[k];
+    const FsItem item = w.items[it];
+    const FsOut o = w.out[it];
+    if (o.status == kFsOk && ii < o.n_seeds && item.rho > 0.0) {
+        const FsSettingsDev st = w.settings[item.settings];
+        Ctx C;
+        C.rays = 0;
+        C.evals = 0;
+        C.budget = 0;
+        FsWork lw{};
+        lw.ld_tables = w.ld_tables;
+        lw.f32_rays = w.f32_rays;
+        init_ctx<W>(C, lw, item, st, nullptr, ld_smem, ld_loaded);
+        const double incr = item.rho / static_cast<double>(max(st.source_bins, 1));
+        C.band = dmax_(4.0 * item.rho * incr, 4.0 * incr * incr);
+        C.step = incr;
+        C.tape_n = 0;
+        R.gen = (epoch << 32) | (0x80000000ull + static_cast<unsigned long long>(e * kSplitSeeds + ii));
+        R.hw = 0;
+        R.ovf = false;
+        rows_ensure<W>(R, 1);
+        const P2 seed = w.seeds[(long long)k * w.seed_cap + ii];
+        if (C.f32) C.A = make_anchor32(C.m, seed.x, seed.y, C.src);
+        const double jseed = jacobian(C.m, seed.x, seed.y);
+        const int js = (fabs(jseed) < 0.02) ? sign_of(jseed) : 0;
+        const SplitUse sp{w.split_info + (long long)e * 2 * kSplitSeeds, w.split_scratch, w.split_bytes, w.seed_cap,
+                          nullptr};
+        const MergeOut mo = merge_halves<W>(R, sp, ii, seed, incr);
+        if (mo.ok) {
+            int yi = mo.yi;
+            R.hw = mo.hw;
+            double areai = mo.areai;
+            C.rays += mo.rays;
+            double mj = 0.0;
+            int reps = 0;
+            const int nyi = repair_walk<W>(C, R, S, js, incr, yi, areai, mo.n_up, mj, reps);
+            Grp<W>::sync();
+            if (!R.ovf && nyi + 1 <= kSplitRowCap) {
+                const RowScratch UR = rows_at(w.split_scratch + (long long)__ldcg(&sp.info[2 * ii].slot) *
+                                                                   w.split_bytes,
+                                              kSplitRowCap, w.seed_cap, nullptr, nullptr);
+                for (int r = t; r <= nyi; r += N) {
+                    UR.xmin[r] = R.xmin[r];
+                    UR.xmax[r] = R.xmax[r];
+                    UR.ax[r] = R.ax[r];
+                    UR.y[r] = R.y[r];
+                    UR.dys[r] = R.dys[r];
+                }
+                out.areai = areai;
+                out.max_jump = mj;
+                out.rays = C.rays;
+                out.nyi = nyi;
+                out.repairs = reps;
+                out.ok = 1;
+            }
+        }
+    }
+    Grp<W>::sync();
+    if (t == 0) w.seed_info[e * kSplitSeeds + ii] = out;
+    return ld_loaded;
+}
+
 // Work items: the list's points in order, each with the group's scratch at
 // `base`.  The early pass with split points (split_info set) takes instead
 // the units of its points, kSplitSeeds seeds by two halves each, in list
@@ -1402,18 +1541,28 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
         if (split) {
             if (idx < n_units) {
                 e = idx / (2 * kSplitSeeds);
-                const UnitArgs ua{w.ir_count + kSplitAlloc, w.split_slots, w.early_cart, w.ir_cart, w.items, w.out, w.settings,
+                const UnitArgs ua{w.ir_count + kSplitAlloc, w.split_slots, w.seed_info, w.early_cart, w.ir_cart, w.items, w.out, w.settings,
                                   w.ld_tables, w.seeds, w.split_scratch, w.split_info, w.split_bytes, w.seed_cap,
                                   w.f32_rays};
-                ld_loaded = run_unit<W>(ua, epoch, e, (idx >> 1) % kSplitSeeds, idx & 1, S, ld_smem, ld_loaded);
+                const int ii = (idx >> 1) % kSplitSeeds;
+                ld_loaded = run_unit<W>(ua, epoch, e, ii, idx & 1, S, ld_smem, ld_loaded);
+                // The second of a seed's halves to complete finishes the seed,
+                // and the last seed of a point to complete finishes the point.
+                __threadfence();
+                Grp<W>::sync();
+                if (t == 0) S.item = atomicAdd(w.ir_count + kSeedCounter + e * kSplitSeeds + ii, 1);
+                Grp<W>::sync();
+                if (S.item != 1) continue;
+                __threadfence();
+                ld_loaded = seed_finish<W>(ua, epoch, e, ii, S, ld_smem, ld_loaded, R);
                 __threadfence();
                 Grp<W>::sync();
                 if (t == 0) S.item = atomicAdd(w.ir_count + kSplitCounter + e, 1);
                 Grp<W>::sync();
-                if (S.item != 2 * kSplitSeeds - 1) continue;
+                if (S.item != kSplitSeeds - 1) continue;
                 __threadfence();
                 su = SplitUse{w.split_info + (long long)e * 2 * kSplitSeeds, w.split_scratch, w.split_bytes,
-                              w.seed_cap};
+                              w.seed_cap, w.seed_info + (long long)e * kSplitSeeds};
                 use = &su;
             } else {
                 e = n_split + (idx - n_units);

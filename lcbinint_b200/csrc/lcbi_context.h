@@ -47,6 +47,7 @@ struct Context {
     unsigned wait_limit = 0;          // polls before a device wait gives up (0: the kernels' default)
     Buffer fs_seed_early;             // seeding of the early points: candidate scratch per warp
     Buffer fs_split, fs_split_info;   // units of the split early points: row scratch and results
+    Buffer fs_seed_info;              // their seeds after the gap repairs
     bool early_live = false;          // the early stream holds work that stage_integrate joins
     bool early_serial = false;        // stage timing on: stage_integrate runs the early block pass
     int seed_block_after = 32;        // in-disk critical sources that move a point's seeding to a block (0: never)
@@ -113,7 +114,7 @@ struct Context {
                           &fs_rays, &fs_retry, &fs_scratch_big, &fs_scratch_polar_big, &fs_cycles, &fs_tiles, &fs_grad_tiles, &fs_grad, &fs_grad_lc,
                           &fs_all_aps, &fs_all_nimg, &pass_raw[0], &pass_raw[1], &pass_branches[0],
                           &pass_branches[1], &pass_lists[0], &pass_lists[1], &pass_counters[0], &pass_counters[1],
-                          &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry, &fs_seed_block, &fs_route, &fs_waits, &fs_seed_early, &fs_split, &fs_split_info,
+                          &pass_jobs[0], &pass_jobs[1], &ir_models, &ir_branches, &ir_lists, &ir_counters, &ir_retry, &fs_seed_block, &fs_route, &fs_waits, &fs_seed_early, &fs_split, &fs_split_info, &fs_seed_info,
                           &fs_needed, &fs_model_base, &fs_tape, &fs_levels})
             v.push_back(b);
         return v;

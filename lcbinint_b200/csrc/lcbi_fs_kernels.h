@@ -150,6 +150,11 @@ struct FsWork {
     long long split_bytes;
     struct SplitInfo* split_info;
     int split_slots;   // row areas in the pool (at most kSplitSlots)
+    // Per seed of a split point (kEarlyMax * kSplitSeeds): the block that
+    // completes a seed's second half (the seed's counter at
+    // ir_count[kSeedCounter + point * kSplitSeeds + seed]) merges the halves,
+    // runs the seed's gap repairs and leaves its rows in the up half's area.
+    struct SeedInfo* seed_info;
 };
 
 constexpr int kEarlyMax = 512;
@@ -164,18 +169,31 @@ struct SplitInfo {
     int slot;                 // its row scratch area
     double row0[3];           // down half: xmin, xmax and y of the first row of the up scan
 };
-constexpr int kSplitSeeds = 4;
+
+// One seed of a split point after its gap repairs.
+struct SeedInfo {
+    double areai;             // the seed's area
+    double max_jump;          // its rows' largest jump, in cells
+    unsigned long long rays;  // its inside cells
+    int nyi;                  // rows [0, nyi] in the up half's area: the walk's row count
+    int repairs;              // its gap repairs
+    int ok;                   // 1: complete; 0: the finishing block scans the seed itself
+    int pad;
+};
+constexpr int kSplitSeeds = 8;
 constexpr int kSplitUnits = kEarlyMax * kSplitSeeds * 2;  // SplitInfo entries
 constexpr int kSplitSlots = 768;                           // unit row scratch areas
 constexpr int kSplitRowCap = 32768;
 // The counters array: ir_count [0, 8), next_item [8, 16), the route's
 // candidate count [48], the unit slots taken [kSplitAlloc], early_cart
-// [kEarlyOff, kEarlyOff + kEarlyMax), completed units per early point
-// [kSplitCounter, kSplitCounter + kEarlyMax).
+// [kEarlyOff, kEarlyOff + kEarlyMax), completed seeds per early point
+// [kSplitCounter, kSplitCounter + kEarlyMax), completed halves per seed
+// [kSeedCounter, kSeedCounter + kEarlyMax * kSplitSeeds).
 constexpr int kSplitAlloc = 49;
 constexpr int kEarlyOff = 64;
 constexpr int kSplitCounter = kEarlyOff + kEarlyMax;
-constexpr int kCounterInts = kSplitCounter + kEarlyMax;
+constexpr int kSeedCounter = kSplitCounter + kEarlyMax;
+constexpr int kCounterInts = kSeedCounter + kEarlyMax * kSplitSeeds;
 constexpr int kEarlyWarps = 4;     // warps per block of the early pass (two blocks per SM)
 constexpr int kEarlyBlocks = 96;   // blocks of the early pass
 

@@ -180,7 +180,7 @@ struct SeedInfo {
     int ok;                   // 1: complete; 0: the finishing block scans the seed itself
     int pad;
 };
-constexpr int kSplitSeeds = 8;
+constexpr int kSplitSeeds = 6;
 constexpr int kSplitUnits = kEarlyMax * kSplitSeeds * 2;  // SplitInfo entries
 constexpr int kSplitSlots = 768;                           // unit row scratch areas
 constexpr int kSplitRowCap = 32768;

@@ -1116,6 +1116,21 @@ def main():
     # steps above run the second Cartesian pass beside the polar passes), so
     # these stage times add up to more than a timed step.
     stage_steps = min(args.steps, 3)
+    # Where each stream of an overlapped step ends (stream marks: timing
+    # events recorded where the early, side and polar streams' work ends,
+    # the overlap unchanged), over further steps.
+    L.lcbi_gpu_set_stream_marks(ctx.handle, 1)
+    marks = []
+    for _ in range(stage_steps):
+        flush_l2(flush)
+        step_device()
+        m = np.zeros(3)
+        L.lcbi_gpu_stream_marks(ctx.handle, _lib.ptr(m), 3)
+        marks.append(m)
+    L.lcbi_gpu_set_stream_marks(ctx.handle, 0)
+    marks = np.median(np.array(marks), axis=0)
+    stream_end_ms = {"early": float(marks[0]), "side": float(marks[1]), "polar": float(marks[2]),
+                     "from": "the start of the seeding stage, median of further overlapped steps"}
     L.lcbi_gpu_set_timing(ctx.handle, 1)
     for _ in range(stage_steps):
         flush_l2(flush)
@@ -1181,6 +1196,7 @@ def main():
                                "figure is half of it (one flop per FP64 instruction)",
                 "achieved_over": "ms_per_step (device-timed steps): counted cells of the step x flop_per_ray",
                 "stage_ms_serialised": {k: v / stage_steps for k, v in shares.items()},
+                "stream_end_ms": stream_end_ms,
                 "stage_timing": f"{stage_steps} further steps with the stages serialised by per-stage events "
                                 "(they overlap on three streams in the timed steps, so they add up to more)",
                 "flop_per_ray": F_RAY}

@@ -64,6 +64,17 @@ int lcbi_gpu_set_timing(lcbi_gpu_context *ctx, int enable);
  * enabled: 0 caustics + limb-darkening tables, 1 decision, 2 seeding,
  * 3 Cartesian inverse ray, 4 polar inverse ray, 5 point source. */
 int lcbi_gpu_stage_times(const lcbi_gpu_context *ctx, double *ms, int64_t *launches, int32_t n);
+/* Enables stream marks (instrumentation, no reference counterpart): every
+ * finite-source call records timing events where its inverse-ray streams end,
+ * without changing how they overlap. */
+int lcbi_gpu_set_stream_marks(lcbi_gpu_context *ctx, int enable);
+/* Device milliseconds from the start of the last call's seeding stage to the
+ * end of, in order, the early stream (the largest Cartesian points' seeding
+ * and block pass), the side stream (the first and second Cartesian passes and
+ * its blocks' share of the early pass) and the context's stream (the polar
+ * passes); -1 for a stream that did not run.  n entries (at most 3) are
+ * written.  Waits for the call's work to finish. */
+int lcbi_gpu_stream_marks(lcbi_gpu_context *ctx, double *ms, int32_t n);
 /* Enables per-point clock64 cycle counts of seeding + inverse-ray integration
  * (instrumentation, read back with lcbi_gpu_last_item_cycles). */
 int lcbi_gpu_set_item_cycles(lcbi_gpu_context *ctx, int enable);
@@ -100,6 +111,12 @@ int lcbi_gpu_set_ray_precision(lcbi_gpu_context *ctx, int32_t bits);
  * fill spread over the whole GPU, 0 the one-warp-per-point segment flood fill.
  * Both count the same cells; results are the same.  No reference counterpart. */
 int lcbi_gpu_set_polar_tiles(lcbi_gpu_context *ctx, int enable);
+/* Load balance of the largest Cartesian points (no reference counterpart):
+ * with 1 (the default), once the first and second Cartesian passes have
+ * finished, their stream's blocks join the early block pass of the points
+ * predicted largest and take the units it has not started; 0 leaves that
+ * pass to its own blocks.  Results are the same for both values. */
+int lcbi_gpu_set_early_helpers(lcbi_gpu_context *ctx, int enable);
 /* Device workspace of the finite-source scans (no reference counterpart):
  * first-pass warps per SM (default 8; about 7 MB of scratch each), second-pass
  * blocks (default 0: one per SM; about 100 MB each; a number set here also

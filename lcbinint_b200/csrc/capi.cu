@@ -64,6 +64,9 @@ Context::~Context()
     if (side_stream) cudaStreamDestroy(side_stream);
     if (early_fork) cudaEventDestroy(early_fork);
     if (early_join) cudaEventDestroy(early_join);
+    if (early_seeded) cudaEventDestroy(early_seeded);
+    for (cudaEvent_t e : marks)
+        if (e) cudaEventDestroy(e);
     if (early_stream) cudaStreamDestroy(early_stream);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -188,6 +191,7 @@ int lcbi_gpu_create(int device, lcbi_gpu_context** out)
         cudaStreamCreateWithPriority(&ctx->early_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->early_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->early_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->early_seeded, cudaEventDisableTiming) != cudaSuccess ||
         cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
@@ -248,6 +252,47 @@ int lcbi_gpu_set_ray_precision(lcbi_gpu_context* c, int32_t bits)
     Context* ctx = reinterpret_cast<Context*>(c);
     if (!ctx || (bits != 32 && bits != 64)) return LCBI_INVALID_ARGUMENT;
     ctx->f32_rays = bits == 32;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_set_stream_marks(lcbi_gpu_context* c, int enable)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    if (enable && ctx->marks[0] == nullptr) {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) return LCBI_GPU_ERROR;
+        for (cudaEvent_t& e : ctx->marks)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                cudaGetLastError();
+                return LCBI_GPU_ERROR;
+            }
+    }
+    ctx->marks_on = enable != 0;
+    ctx->marks_set = 0;
+    return LCBI_OK;
+}
+
+int lcbi_gpu_stream_marks(lcbi_gpu_context* c, double* ms, int32_t n)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || !ms || n < 0) return LCBI_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return LCBI_GPU_ERROR;
+    for (int i = 0; i < n && i < 3; ++i) {
+        ms[i] = -1.0;
+        float f = 0.0f;
+        if ((ctx->marks_set & 1u) && (ctx->marks_set & (2u << i)) &&
+            cudaEventSynchronize(ctx->marks[i + 1]) == cudaSuccess &&
+            cudaEventElapsedTime(&f, ctx->marks[0], ctx->marks[i + 1]) == cudaSuccess)
+            ms[i] = f;
+    }
+    return LCBI_OK;
+}
+
+int lcbi_gpu_set_early_helpers(lcbi_gpu_context* c, int enable)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx) return LCBI_INVALID_ARGUMENT;
+    ctx->early_helpers = enable != 0;
     return LCBI_OK;
 }
 

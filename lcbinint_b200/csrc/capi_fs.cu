@@ -387,6 +387,8 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
     if (ctx->early_live && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
     if (!next_epoch(ctx)) return false;
     ctx->early_live = false;
+    ctx->marks_set = 0;
+    ctx->mark(0, ctx->stream);
     ctx->early_serial = false;
     // Candidate keys and probes share one allocation: all warps' keys, then all probes.
     const size_t per = seed_candidate_bytes_per_warp(ctx->cand_cap);
@@ -411,10 +413,12 @@ bool stage_seeds(Context* ctx, const FsWork& w, int max_points)
                 return false;
             const bool ok =
                 ctx->check("seeds early", launch_seeds(es, ctx->sm_count, ctx->early_stream, ek, ep, kEarlyMax)) &&
+                ctx->check("early seeded", cudaEventRecord(ctx->early_seeded, ctx->early_stream)) &&
                 ctx->check("cartesian early",
                            launch_cartesian(early_work(ctx, w), early_blocks(ctx), ctx->early_stream, ctx->epoch));
             // Recorded even after a failed launch: the context's stream must
             // never run ahead of work already queued beside it.
+            ctx->mark(1, ctx->early_stream);
             if (!ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream))) return false;
             ctx->early_live = true;
             if (!ok) return false;
@@ -489,11 +493,28 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         if (!ctx->check("fork", cudaEventRecord(ctx->fork_event, ctx->stream)) ||
             !ctx->check("fork", cudaStreamWaitEvent(ctx->side_stream, ctx->fork_event, 0)))
             return false;
-        const bool ok =
+        bool ok =
             ctx->check("cartesian", launch_cartesian(w, warps, ctx->side_stream, ctx->epoch)) &&
             ctx->check("cartesian retry", launch_cartesian(r, retry_blocks(ctx), ctx->side_stream, ctx->epoch));
+        // Then the side stream's blocks join the early pass: the early pass's
+        // units and points are claimed from one counter, so blocks launched
+        // later take whatever is left, and the SMs the first and second passes
+        // leave idle scan early units instead of waiting for the early
+        // stream's blocks.  They use the second pass's scratch areas, free
+        // once it has finished on this stream, with row-key generations above
+        // the second pass's.  Which block runs a unit does not change its
+        // result.
+        if (ok && ctx->early_live && ctx->early_helpers) {
+            FsWork h = early_work(ctx, w);
+            h.scratch = static_cast<char*>(ctx->fs_scratch_big.ptr);
+            h.gen_base = 0x40000000u;
+            ok = ctx->check("early seeded", cudaStreamWaitEvent(ctx->side_stream, ctx->early_seeded, 0)) &&
+                 ctx->check("cartesian early", launch_cartesian(h, retry_blocks(ctx), ctx->side_stream, ctx->epoch));
+            ctx->launches += 1;
+        }
         // The join is recorded even after a failed launch, so that the
         // context's stream never runs ahead of work already queued beside it.
+        ctx->mark(2, ctx->side_stream);
         if (!ctx->check("join", cudaEventRecord(ctx->join_event, ctx->side_stream)) || !ok) return false;
     }
     ctx->stage_begin(4, &ev);
@@ -515,6 +536,7 @@ bool stage_integrate(Context* ctx, const FsWork& w, int max_points)
         polar_ok = ctx->check("polar retry", launch_polar(r, retry_blocks(ctx), ctx->stream, ctx->epoch));
         ctx->stage_end(4, ev);
     }
+    ctx->mark(3, ctx->stream);
     if (overlap && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0))) return false;
     if (ctx->early_live && !ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0))) return false;
     ctx->early_live = false;

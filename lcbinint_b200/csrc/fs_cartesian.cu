@@ -1522,7 +1522,7 @@ __device__ void cartesian_body(const FsWork& w, unsigned long long epoch, CartLi
     double* areaimage;
     int* flags;
     RowScratch R = rows_at(base, cap, w.seed_cap, &areaimage, &flags);
-    unsigned long long local_gen = 0;
+    unsigned long long local_gen = w.gen_base;
     const int n = *L.count;
     const bool split = w.early_pass && w.split_info != nullptr && L.slots != nullptr;
     const int n_split = split ? min(n, kEarlyMax) : 0;
@@ -1702,11 +1702,13 @@ __global__ void __launch_bounds__(32 * kBigWarps, 1) cartesian_block_kernel(FsWo
                               w.tape ? w.tape + (long long)blockIdx.x * kTapeMax : nullptr, ld_smem);
 }
 
-// The early pass: blocks of kEarlyWarps warps, two per SM.  Its work is the
+// The early pass: blocks of kEarlyWarps warps, one per SM.  Its work is the
 // split points' seed-half units, each a serial row scan whose speed is set
-// by latency, not by the SM's issue rate, so two smaller groups per SM scan
-// about twice the rows of one large group in the same time.
-__global__ void __launch_bounds__(32 * kEarlyWarps, 2) cartesian_early_kernel(FsWork w, unsigned long long epoch)
+// by latency, not by the SM's issue rate.  The point's limb-darkening table
+// in shared memory (160 KB) leaves room for one block per SM; blocks without
+// it (two per SM, the entries evaluated where needed or read through L1) were
+// measured no faster on the 4,096-point batch.
+__global__ void __launch_bounds__(32 * kEarlyWarps, 1) cartesian_early_kernel(FsWork w, unsigned long long epoch)
 {
     __shared__ CartShared<kEarlyWarps> sh;
     extern __shared__ double ld_smem[];

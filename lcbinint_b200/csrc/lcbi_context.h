@@ -69,6 +69,7 @@ struct Context {
     long long cell_budget = 1 << 19;
     bool cell_budget_set = false;  // set by the caller; else small batches send every point to blocks
     int retry_blocks = 0;      // 0: one per SM
+    bool early_helpers = true;  // the side stream's blocks join the early pass after the Cartesian passes
     int row_cap_big = 1 << 19;
     int queue_cap_big = 1 << 19;
     int hash_cap_big = 1 << 21;
@@ -90,6 +91,19 @@ struct Context {
     // blocks from the start, beside the first pass.
     cudaStream_t early_stream = nullptr;
     cudaEvent_t early_fork = nullptr, early_join = nullptr;
+    // Recorded on the early stream once the early points are seeded: the
+    // side stream waits for it before its own blocks join the early pass.
+    cudaEvent_t early_seeded = nullptr;
+    // Stream marks (lcbi_gpu_set_stream_marks): timing events at the start of
+    // the seeding stage [0] and where the early [1], side [2] and context [3]
+    // streams' inverse-ray work ends; bit i of marks_set: event i recorded.
+    bool marks_on = false;
+    cudaEvent_t marks[4] = {};
+    unsigned marks_set = 0;
+    void mark(int i, cudaStream_t s)
+    {
+        if (marks_on && marks[i] != nullptr && cudaEventRecord(marks[i], s) == cudaSuccess) marks_set |= 1u << i;
+    }
 
     // Optional per-stage kernel timing with CUDA events on the launch stream.
     static constexpr int kStages = 8;  // 0 caustics+LD, 1 decide, 2 seeds, 3 cartesian, 4 polar, 5 point source

@@ -155,6 +155,11 @@ struct FsWork {
     // ir_count[kSeedCounter + point * kSplitSeeds + seed]) merges the halves,
     // runs the seed's gap repairs and leaves its rows in the up half's area.
     struct SeedInfo* seed_info;
+    // Row-key generations of this launch's scans start above gen_base, so a
+    // launch whose blocks reuse scratch areas that an earlier launch of the
+    // same epoch scanned in (the side stream's blocks joining the early pass
+    // in the second pass's areas) never takes that launch's rows for its own.
+    unsigned gen_base;
 };
 
 constexpr int kEarlyMax = 512;
@@ -194,7 +199,7 @@ constexpr int kEarlyOff = 64;
 constexpr int kSplitCounter = kEarlyOff + kEarlyMax;
 constexpr int kSeedCounter = kSplitCounter + kEarlyMax;
 constexpr int kCounterInts = kSeedCounter + kEarlyMax * kSplitSeeds;
-constexpr int kEarlyWarps = 4;     // warps per block of the early pass (two blocks per SM)
+constexpr int kEarlyWarps = 4;     // warps per block of the early pass (one block per SM: its LD table)
 constexpr int kEarlyBlocks = 96;   // blocks of the early pass
 
 constexpr int kBigWarps = 8;

@@ -6,10 +6,12 @@
 //
 // One thread solves one polynomial.  The largest degree is a template
 // parameter so every Horner loop unrolls and all coefficients stay in
-// registers; the solves of the deflation degrees run as one loop of
-// evaluations (deflation_chain), so the lanes of a warp share them whatever
-// regime or degree each lane is in.  Each regime is bounded (80 steps, as in
-// the method), so a solve always terminates.
+// registers.  The quintic's solves of the deflation degrees run as one loop
+// of evaluations (deflation_chain), so the lanes of a warp share them whatever
+// regime or degree each lane is in; the quartic's run as the method's loops,
+// one degree after the other (laguerre2newton, deflate_step).  Both forms make
+// the same steps.  Each regime is bounded (80 steps, as in the method), so a
+// solve always terminates.
 #pragma once
 
 #include "lcbi_complex.cuh"
@@ -374,6 +376,171 @@ __device__ __forceinline__ void newton_polish(const dc* poly, dc& root)
     }
 }
 
+// Three-regime solver (cmplx_laguerre2newton, SkowronGould.cpp:764-1130) for
+// one degree, its regimes as three loops run in turn, starting in Laguerre
+// mode from `root`.  Returns false on non-convergence.  The quartic solves of
+// the caustic sampling use this form: the phases a warp takes lie side by side
+// on one critical curve and need about as many steps each, so the fused loop
+// of deflation_chain saves them little and costs its predicated steps
+// (caustic sampling of the 1,024-model orbital batch: 577 ms with this form,
+// 630 ms fused).
+template <int N>
+__device__ __forceinline__ bool laguerre2newton(const dc* poly, dc& root)
+{
+    const double one_nth = 1.0 / N;
+    const double n_1_nth = (N - 1) * one_nth;
+    const double two_n_div_n_1 = 2.0 / n_1_nth;
+    int iter = 0;
+    double cr = 0.0;
+    int j = 1;
+    bool good = false;
+    int mode = 2;
+    // Each pass of this loop runs at most 80 + 80 + 11 steps and adds at least
+    // one to `iter`; the Newton regime leaves with failure once iter >= 80.
+    for (int guard = 0; guard < 64; ++guard) {
+        if (mode >= 2) {
+            int i;
+            for (i = 1; i <= kMaxIt; ++i) {
+                dc p, dp, d2;
+                double ek;
+                horner<N, true>(poly, root, p, dp, d2, ek, true);
+                const double abs2p = cnorm2(p);
+                ++iter;
+                if (abs2p == 0.0) return true;
+                cr = crit2(ek);
+                if (abs2p < cr) {
+                    if (abs2p < 0.01 * cr) return true;
+                    good = true;
+                } else {
+                    good = false;
+                }
+                dc denom{0.0, 0.0}, fn{0.0, 0.0};
+                if (!czero(dp)) {
+                    fn = cdiv(p, dp);
+                    const dc fe = cdiv(d2, dp);
+                    const dc fh = cmul(fn, fe);
+                    const double a2f = cnorm2(fh);
+                    if (a2f <= 0.0625) mode = (a2f <= 0.000625) ? 0 : 1;
+                    const dc t = cscale(two_n_div_n_1, fh);
+                    const dc ds = csqrt_sg(dc{1.0 - t.re, 0.0 - t.im});
+                    const dc nd = cscale(n_1_nth, ds);
+                    denom = (ds.re > 0.0) ? dc{one_nth + nd.re, 0.0 + nd.im} : dc{one_nth - nd.re, 0.0 - nd.im};
+                }
+                dc dx;
+                if (czero(denom)) {
+                    const dc e = escape_dir(jump(i % 10) * 2 * 3.14159265358979323846);
+                    dx = dc{(cabs_(root) + 1.0) + e.re, e.im};
+                } else {
+                    dx = cdiv(fn, denom);
+                }
+                dc nr = csub(root, dx);
+                if (ceq(nr, root)) return true;
+                if (good) { root = nr; return true; }
+                if (mode != 2) {
+                    root = nr;
+                    j = i + 1;
+                    break;
+                }
+                if (i % 10 == 0) nr = csub(root, cscale(jump((i / 10 - 1) % 10), dx));
+                root = nr;
+            }
+            if (i >= kMaxIt) return false;
+        }
+        if (mode == 1) {
+            int i;
+            for (i = j; i <= kMaxIt; ++i) {
+                const bool fresh = ((i - j) % 10 == 0);
+                dc p, dp, d2;
+                double ek;
+                horner<N, true>(poly, root, p, dp, d2, ek, fresh);
+                if (fresh) cr = crit2(ek);
+                const double abs2p = cnorm2(p);
+                ++iter;
+                if (abs2p == 0.0) return true;
+                if (abs2p < cr) {
+                    if (czero(dp)) return true;
+                    if (abs2p < 0.01 * cr) return true;
+                    good = true;
+                } else {
+                    good = false;
+                }
+                dc dx;
+                if (czero(dp)) {
+                    dx = cscale(cabs_(root) + 1.0, escape_dir(jump(i % 10) * 2 * 3.14159265358979323846));
+                } else {
+                    const dc fn = cdiv(p, dp);
+                    const dc fe = cdiv(d2, dp);
+                    const dc fh = cmul(fn, fe);
+                    if (cnorm2(fh) <= 0.000625) mode = 0;
+                    dx = cmul(fn, dc{1.0 + fh.re, 0.0 + fh.im});
+                }
+                dc nr = csub(root, dx);
+                if (ceq(nr, root)) return true;
+                if (good) { root = nr; return true; }
+                if (mode != 1) {
+                    root = nr;
+                    j = i + 1;
+                    break;
+                }
+                if (i % 10 == 0) nr = csub(root, cscale(jump((i / 10 - 1) % 10), dx));
+                root = nr;
+            }
+            if (i >= kMaxIt) return false;
+        }
+        if (mode == 0) {
+            for (int i = j; i <= j + 10; ++i) {
+                const bool fresh = (i == j);
+                dc p, dp, d2;
+                double ek;
+                horner<N, false>(poly, root, p, dp, d2, ek, fresh);
+                if (fresh) cr = crit2(ek);
+                const double abs2p = cnorm2(p);
+                ++iter;
+                if (abs2p == 0.0) return true;
+                if (abs2p < cr) {
+                    if (czero(dp)) return true;
+                    if (abs2p < 0.01 * cr) return true;
+                    good = true;
+                } else {
+                    good = false;
+                }
+                dc dx;
+                if (czero(dp)) dx = cscale(cabs_(root) + 1.0, escape_dir(2 * 3.14159265358979323846 * jump(i % 10)));
+                else dx = cdiv(p, dp);
+                const dc nr = csub(root, dx);
+                if (ceq(nr, root)) return true;
+                if (good) { root = nr; return true; }
+                root = nr;
+            }
+            if (iter >= kMaxIt) return false;
+            mode = 2;
+        }
+    }
+    return false;
+}
+
+// Find one root of the degree-N leading block of p2 from a cold start, then
+// divide it out in place (SkowronGould.cpp:123-155).
+template <int N>
+__device__ __forceinline__ dc deflate_step(dc* p2)
+{
+    dc root{0.0, 0.0};
+    if (!laguerre2newton<N>(p2, root)) {
+        PolyN<N> pn;
+#pragma unroll
+        for (int i = 0; i <= N; ++i) pn.c[i] = p2[i];
+        root = laguerre_fallback<N>(pn, dc{0.0, 0.0});
+    }
+    dc coef = p2[N];
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+        const dc prev = p2[i];
+        p2[i] = coef;
+        coef = cadd(prev, cmul(root, coef));
+    }
+    return root;
+}
+
 // Direct quadratic tail (solve_quadratic_eq, SkowronGould.cpp:1132-1154).
 __device__ __forceinline__ void quadratic(dc& x0, dc& x1, const dc* poly)
 {
@@ -433,7 +600,8 @@ __device__ __forceinline__ void roots4(const dc* poly, dc* roots)
     sg::PolyN<4> pn;
 #pragma unroll
     for (int i = 0; i < 5; ++i) p2[i] = pn.c[i] = poly[i];
-    sg::deflation_chain<4>(p2, roots);
+    roots[3] = sg::deflate_step<4>(p2);
+    roots[2] = sg::deflate_step<3>(p2);
     sg::quadratic(roots[1], roots[0], p2);
 #pragma unroll
     for (int n = 0; n < 3; ++n) roots[n] = sg::polish_root<4>(pn, roots[n]);

@@ -126,3 +126,36 @@ def test_early_block_routing_keeps_results():
     assert (base["method"] == 2).any()
     for budget in (1 << 12, 1 << 19):
         assert outs[budget].tobytes() == base.tobytes(), budget
+
+
+def test_early_helpers_match_the_early_pass_alone():
+    """Once the Cartesian passes on the side stream are done, that stream's
+    blocks join the early block pass of the largest points and take the units
+    it has not started.  With eight second-pass blocks the early pass also has
+    eight blocks, so the 4,096-point batch leaves the joining blocks most of
+    the early units; the results must be the bytes of the early pass alone."""
+    import bench
+    from lcbinint_b200 import _lib
+    from lcbinint_b200.api import FS_POINT_DTYPE, FS_RESULT_DTYPE, LcbiStructs, PS_EXACT, PS_ON_DEVICE
+    rows = bench.fs_batch_workload(seed=1)
+    settings, sidx = bench.fs_settings_for(rows)
+    st = (LcbiStructs.FsSettings * len(settings))(*settings)
+    pts = np.zeros(len(rows), dtype=FS_POINT_DTYPE)
+    pts["s"], pts["q"], pts["y1"], pts["y2"], pts["rho"] = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
+    pts["settings"] = sidx
+    pts["flags"] = PS_EXACT | PS_ON_DEVICE
+    ctx = _lib.Context(0)
+    L = ctx._L
+    assert L.lcbi_gpu_set_workspace(ctx.handle, 0, 8, 0) == 0
+
+    def run(helpers):
+        assert L.lcbi_gpu_set_early_helpers(ctx.handle, helpers) == 0
+        out = np.zeros(len(rows), dtype=FS_RESULT_DTYPE)
+        ctx.check(L.lcbi_gpu_binary_mag(ctx.handle, st, len(settings), None, 0, len(rows), pts.ctypes.data,
+                                        out.ctypes.data, 0), "lcbi_gpu_binary_mag")
+        return out
+
+    alone = run(0)
+    assert (alone["status"] == 0).all()
+    for _ in range(2):
+        assert run(1).tobytes() == alone.tobytes()

@@ -9,7 +9,7 @@
 
 namespace lcbi {
 
-__global__ void __launch_bounds__(128, 5) ps_batch_kernel(const double* __restrict__ s, const double* __restrict__ q,
+__global__ void __launch_bounds__(128, 4) ps_batch_kernel(const double* __restrict__ s, const double* __restrict__ q,
                                                       const double* __restrict__ y1, const double* __restrict__ y2,
                                                       double* __restrict__ A, int* __restrict__ nimg,
                                                       int* __restrict__ status, long long n)

@@ -165,7 +165,71 @@ template bool Context::stage_out<int>(Buffer&, int*, size_t, bool, int**);
 template bool Context::copy_back<double>(double*, const double*, size_t, bool);
 template bool Context::copy_back<int>(int*, const int*, size_t, bool);
 
+// Point-source batches from host memory of at least two chunks: chunks of
+// kPsChunk positions go round-robin to the context's three streams, each
+// chunk's copies in, kernel and copies out in order on its stream, so the
+// copies of some chunks run on the copy engines while the kernels of others
+// run on the SMs.  Every position's result is the kernel's, so the results
+// are those of one launch over the whole batch.  (With pinned host memory
+// the copies are asynchronous; pageable memory still gives correct results,
+// with less overlap.)
+constexpr size_t kPsChunk = size_t(1) << 18;
+
+int ps_pipelined(Context* ctx, size_t N, const double* s, const double* q, const double* y1, const double* y2,
+                 double* A, int32_t* image_count, int32_t* status)
+{
+    if (!ctx->ensure(ctx->in[0], N * sizeof(double)) || !ctx->ensure(ctx->in[1], N * sizeof(double)) ||
+        !ctx->ensure(ctx->in[2], N * sizeof(double)) || !ctx->ensure(ctx->in[3], N * sizeof(double)) ||
+        !ctx->ensure(ctx->out[0], N * sizeof(double)) ||
+        (image_count && !ctx->ensure(ctx->out[1], N * sizeof(int))) ||
+        (status && !ctx->ensure(ctx->out[2], N * sizeof(int))))
+        return LCBI_GPU_ERROR;
+    cudaStream_t streams[3] = {ctx->stream, ctx->side_stream, ctx->early_stream};
+    if (!ctx->check("fork", cudaEventRecord(ctx->fork_event, ctx->stream)) ||
+        !ctx->check("fork", cudaStreamWaitEvent(ctx->side_stream, ctx->fork_event, 0)) ||
+        !ctx->check("fork", cudaStreamWaitEvent(ctx->early_stream, ctx->fork_event, 0)))
+        return LCBI_GPU_ERROR;
+    const double* hin[4] = {s, q, y1, y2};
+    bool ok = true;
+    size_t c = 0;
+    for (size_t off = 0; off < N && ok; off += kPsChunk, ++c) {
+        const size_t m = N - off < kPsChunk ? N - off : kPsChunk;
+        cudaStream_t st = streams[c % 3];
+        double* din[4];
+        for (int k = 0; k < 4 && ok; ++k) {
+            din[k] = static_cast<double*>(ctx->in[k].ptr) + off;
+            ok = ctx->check("cudaMemcpyAsync H2D",
+                            cudaMemcpyAsync(din[k], hin[k] + off, m * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        double* dA = static_cast<double*>(ctx->out[0].ptr) + off;
+        int* dn = image_count ? static_cast<int*>(ctx->out[1].ptr) + off : nullptr;
+        int* dst = status ? static_cast<int*>(ctx->out[2].ptr) + off : nullptr;
+        ok = ok && ctx->check("ps_batch_kernel", launch_ps_batch(din[0], din[1], din[2], din[3], dA, dn, dst,
+                                                                 static_cast<long long>(m), ctx->sm_count, st));
+        ok = ok && ctx->check("cudaMemcpyAsync D2H",
+                              cudaMemcpyAsync(A + off, dA, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (dn)
+            ok = ok && ctx->check("cudaMemcpyAsync D2H", cudaMemcpyAsync(image_count + off, dn, m * sizeof(int),
+                                                                         cudaMemcpyDeviceToHost, st));
+        if (dst)
+            ok = ok && ctx->check("cudaMemcpyAsync D2H",
+                                  cudaMemcpyAsync(status + off, dst, m * sizeof(int), cudaMemcpyDeviceToHost, st));
+        ctx->launches += 1;
+    }
+    // Joined even after a failure, so the context's stream never runs ahead
+    // of work queued beside it.
+    const bool joined = ctx->check("join", cudaEventRecord(ctx->join_event, ctx->side_stream)) &&
+                        ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->join_event, 0)) &&
+                        ctx->check("join", cudaEventRecord(ctx->early_join, ctx->early_stream)) &&
+                        ctx->check("join", cudaStreamWaitEvent(ctx->stream, ctx->early_join, 0));
+    if (!joined || !ctx->finish() || !ok) return LCBI_GPU_ERROR;
+    return LCBI_OK;
+}
+
 } // namespace lcbi
+
+using lcbi::kPsChunk;
+using lcbi::ps_pipelined;
 
 extern "C" {
 
@@ -377,6 +441,7 @@ int lcbi_gpu_binary_mag0(lcbi_gpu_context* c, int64_t n, const double* s, const 
     cudaSetDevice(ctx->device);
     const bool dev = (flags & LCBI_GPU_DEVICE_POINTERS) != 0;
     const size_t N = static_cast<size_t>(n);
+    if (!dev && !ctx->timing && N >= 2 * kPsChunk) return ps_pipelined(ctx, N, s, q, y1, y2, A, image_count, status);
     const double *ds, *dq, *dy1, *dy2;
     double* dA;
     int *dn, *dst;

@@ -95,3 +95,53 @@ def test_full_size_properties():
     assert (A >= 1.0 - 1e-12).all()
     B = lb.binary_mag0_batch(s, q, y1, -y2)
     assert np.max(np.abs(A / B - 1.0)) < 1e-9
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_batch_pipeline_matches_device_pointers(oracle_lib, pinned):
+    """Host-memory batches of two or more 262,144-position chunks run chunk by
+    chunk on three streams (copies beside kernels); magnifications, image
+    counts and statuses must be the bytes of one device-pointer launch, and a
+    sample must match the oracle.  700,001 positions: two full chunks and a
+    ragged third, with degenerate positions (s = 0, q = 0, source on the
+    lighter lens) spread through it."""
+    import torch
+    import lcbinint_b200 as lb
+    from lcbinint_b200 import _lib
+    n = 700_001
+    s, q, y1, y2 = (np.ascontiguousarray(v) for v in _cfg2_points(n, 7))
+    s[::99_991] = 0.0
+    q[5::123_457] = 0.0
+    s[7], q[7], y2[7] = 1.5, 0.5, 0.0
+    y1[7] = -((-s[7]) * (1.0 / (1.0 + q[7])))  # source exactly on the lighter lens: NaN, status 2
+    ctx = lb.context()
+    L = ctx._L
+    host_in = [s, q, y1, y2]
+    if pinned:
+        host_in = [torch.from_numpy(a).pin_memory() for a in host_in]
+        A = torch.empty(n, dtype=torch.float64).pin_memory()
+        nimg = torch.empty(n, dtype=torch.int32).pin_memory()
+        st = torch.empty(n, dtype=torch.int32).pin_memory()
+        ptrs = [t.data_ptr() for t in host_in] + [A.data_ptr(), nimg.data_ptr(), st.data_ptr()]
+    else:
+        A = np.empty(n); nimg = np.empty(n, dtype=np.int32); st = np.empty(n, dtype=np.int32)
+        ptrs = [_lib.ptr(a) for a in host_in] + [_lib.ptr(A), _lib.ptr(nimg), _lib.ptr(st)]
+    ctx.check(L.lcbi_gpu_binary_mag0(ctx.handle, n, *ptrs, 0), "lcbi_gpu_binary_mag0 (host)")
+    dev = [torch.from_numpy(a).cuda() for a in (s, q, y1, y2)]
+    dA = torch.empty(n, dtype=torch.float64, device="cuda")
+    dn = torch.empty(n, dtype=torch.int32, device="cuda")
+    ds = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.check(L.lcbi_gpu_binary_mag0(ctx.handle, n, *[t.data_ptr() for t in dev], dA.data_ptr(), dn.data_ptr(),
+                                     ds.data_ptr(), 1), "lcbi_gpu_binary_mag0 (device)")
+    A, nimg, st = (np.asarray(v) for v in (A, nimg, st))
+    assert A.view(np.int64).tobytes() == dA.cpu().numpy().view(np.int64).tobytes()
+    assert np.array_equal(nimg, dn.cpu().numpy())
+    assert np.array_equal(st, ds.cpu().numpy())
+    assert st[7] == 2 and (st == 0).sum() == n - 1
+    assert np.isnan(A[7]) and A[0] == 0.0 and A[5] == 0.0
+    idx = np.random.default_rng(3).choice(n, 20_000, replace=False)
+    idx = np.union1d(idx, [n - 1])
+    idx = idx[(s[idx] != 0.0) & (q[idx] != 0.0) & (idx != 7)]
+    Ao, no = oracle_lib.binary_mag0(s[idx], q[idx], y1[idx], y2[idx])
+    assert np.array_equal(A[idx].view(np.int64), Ao.view(np.int64))
+    assert np.array_equal(nimg[idx], no)

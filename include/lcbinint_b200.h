@@ -122,7 +122,7 @@ int lcbi_gpu_set_early_helpers(lcbi_gpu_context *ctx, int enable);
  * blocks (default 0: one per SM; about 100 MB each; a number set here also
  * sets the early pass of the largest Cartesian points to as many blocks, at
  * least 2 and at most 96, of 40 MB each, with 32 unit row areas of 2.5 MB per
- * block, at most 768) and the polar tile table's
+ * block, at most 256) and the polar tile table's
  * capacity (a power of two, default 1048576 tiles of 400 B).  Smaller values
  * trade speed for memory; results do not change.  A value <= 0 keeps the
  * current setting, except second-pass blocks, where 0 means one per SM. */

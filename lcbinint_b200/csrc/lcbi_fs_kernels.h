@@ -187,7 +187,7 @@ struct SeedInfo {
 };
 constexpr int kSplitSeeds = 6;
 constexpr int kSplitUnits = kEarlyMax * kSplitSeeds * 2;  // SplitInfo entries
-constexpr int kSplitSlots = 768;                           // unit row scratch areas
+constexpr int kSplitSlots = 256;                           // unit row scratch areas (see split_slots)
 constexpr int kSplitRowCap = 32768;
 // The counters array: ir_count [0, 8), next_item [8, 16), the route's
 // candidate count [48], the unit slots taken [kSplitAlloc], early_cart

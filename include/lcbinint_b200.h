@@ -305,7 +305,10 @@ int lcbi_gpu_light_curves(lcbi_gpu_context *ctx, const lcbi_fs_settings *setting
  * at rho and six Gauss-Legendre radii, which carry the limb-darkening term
  * without its interior singularity, on a lattice of rho/48 cells (slot 6 holds
  * the continuum value); quadratic limb darkening (d != 0) adds six radii
- * rho sqrt(1 - u^4) at Gauss-Legendre nodes u of [0, 1]. */
+ * rho sqrt(1 - u^4) at Gauss-Legendre nodes u of [0, 1].  The contour sums
+ * are accumulated with FP64 atomic additions in an order that varies between
+ * calls, so inverse-ray gradients repeat to rounding, not bit for bit (the
+ * magnifications do repeat bit for bit). */
 int lcbi_gpu_binary_mag_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *settings, int32_t n_settings,
                              const lcbi_lens_model *models, int32_t n_models, int64_t n,
                              const lcbi_fs_point *points, lcbi_fs_result *results, double *grads,

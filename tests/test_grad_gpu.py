@@ -205,8 +205,11 @@ def test_light_curve_autograd_matches_finite_differences():
 
 def test_device_resident_autograd_matches_the_host_arrays():
     """Times, magnifications and gradients as CUDA tensors
-    (lcbi_gpu_light_curves_grad_device) give the host path's values bit for
-    bit, and torch.autograd runs through them on the device."""
+    (lcbi_gpu_light_curves_grad_device) give the host path's magnifications
+    bit for bit, and torch.autograd runs through them on the device.  The
+    inverse-ray gradients are sums that the gradient flood fill accumulates
+    with FP64 atomic additions, whose order varies from run to run, so two
+    runs agree to rounding of the summed magnitudes, not bit for bit."""
     import torch
     from lcbinint_b200.autograd import light_curve_magnification, light_curves_with_grad
     P = np.array([[0.0, 1.0, -0.01, 0.5, 0.95, 0.01, 5e-3, 0.5], [0.1, 20.0, 0.3, 0.7, 1.3, 0.01, 1e-3, 0.4],
@@ -227,7 +230,12 @@ def test_device_resident_autograd_matches_the_host_arrays():
     got = params.grad.cpu().numpy()
     fin = np.isfinite(want)
     assert np.array_equal(np.isfinite(got), fin)
-    assert np.allclose(got[fin], want[fin], rtol=1e-12, atol=0)
+    # Rounding of a sum depends on its order: bound the difference by 1e-11 of
+    # the magnitudes summed (the weighted per-epoch gradients), plus 1e-12
+    # relative.
+    scale = (np.abs(np.nan_to_num(dA, nan=0.0, posinf=0.0, neginf=0.0)) * np.arange(64)[None, :, None]).sum(axis=1)
+    diff = np.abs(got[fin] - want[fin])
+    assert (diff <= 1e-12 * np.abs(want[fin]) + 1e-11 * scale[fin]).all(), np.max(diff / (scale[fin] + 1e-300))
 
 
 @pytest.mark.parametrize("mode", [1, 2])

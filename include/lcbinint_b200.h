@@ -314,6 +314,16 @@ int lcbi_gpu_binary_mag_grad(lcbi_gpu_context *ctx, const lcbi_fs_settings *sett
                              const lcbi_fs_point *points, lcbi_fs_result *results, double *grads,
                              unsigned flags);
 
+/* Resolution of the inverse-ray gradients' lattice (no reference
+ * counterpart): cells of rho / cells_per_radius (default 48, accepted 8 to
+ * 512).  The gradient is that of a piecewise-linear approximation of the
+ * continuum magnification on this lattice, whose error falls as the square
+ * of the cell, so a finer lattice brings the gradient (and the continuum
+ * value in its slot 6) closer to the continuum's; time and tile-table use
+ * grow as the square of cells_per_radius, and a point whose tiles do not fit
+ * the table gets NaN gradients. */
+int lcbi_gpu_set_grad_resolution(lcbi_gpu_context *ctx, int32_t cells_per_radius);
+
 /* Light curves with gradients: params[m] = {t0, tE, u0, alpha, s, q, rho,
  * Gamma} (VBM convention, Gamma the linear limb-darkening coefficient, which
  * replaces settings->limb_darkening_c per model); A[n_times] and, if dA is not

@@ -131,6 +131,8 @@ def _declare(L):
     L.lcbi_gpu_set_seed_block_after.restype = C.c_int
     L.lcbi_gpu_set_ray_precision.argtypes = [_vp, C.c_int32]
     L.lcbi_gpu_set_ray_precision.restype = C.c_int
+    L.lcbi_gpu_set_grad_resolution.argtypes = [_vp, C.c_int32]
+    L.lcbi_gpu_set_grad_resolution.restype = C.c_int
     L.lcbi_gpu_set_stream_marks.argtypes = [_vp, C.c_int]
     L.lcbi_gpu_set_stream_marks.restype = C.c_int
     L.lcbi_gpu_stream_marks.argtypes = [_vp, _vp, C.c_int32]

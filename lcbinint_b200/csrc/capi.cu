@@ -319,6 +319,14 @@ int lcbi_gpu_set_ray_precision(lcbi_gpu_context* c, int32_t bits)
     return LCBI_OK;
 }
 
+int lcbi_gpu_set_grad_resolution(lcbi_gpu_context* c, int32_t cells_per_radius)
+{
+    Context* ctx = reinterpret_cast<Context*>(c);
+    if (!ctx || cells_per_radius < 8 || cells_per_radius > 512) return LCBI_INVALID_ARGUMENT;
+    ctx->grad_bins = cells_per_radius;
+    return LCBI_OK;
+}
+
 int lcbi_gpu_set_stream_marks(lcbi_gpu_context* c, int enable)
 {
     Context* ctx = reinterpret_cast<Context*>(c);

@@ -280,3 +280,40 @@ def test_quadratic_limb_darkening_gradient_matches_its_continuum_value(mode):
         fd = (ru["magnification"] - rd["magnification"]) / (2 * h)
         err = np.abs(g[:, 4] - fd) * rho / A
         assert np.median(err) < 3e-2, (np.median(err), np.max(err))
+
+
+def test_inverse_ray_gradient_converges_with_its_lattice():
+    """The inverse-ray gradient is that of a piecewise-linear approximation on
+    a lattice of rho / cells cells (lcbi_gpu_set_grad_resolution), whose error
+    falls as the square of the cell: on near-caustic points the gradients and
+    the continuum value at 48 and 96 cells per radius approach those at 192,
+    the 96-cell ones closer (median over points and parameters)."""
+    from lcbinint_b200 import _lib
+    rows = _near_caustic(16, seed=21, rho_range=(3e-3, 1e-2), spread=1.0)
+    st = [_settings(mode=1, nbin=50, c=0.4, forced_ir=True)]
+    sidx = np.zeros(len(rows))
+    ctx = _lib.context(0)
+    out = {}
+    try:
+        for cells in (48, 96, 192):
+            assert ctx._L.lcbi_gpu_set_grad_resolution(ctx.handle, cells) == 0
+            res, g = _run(np.column_stack([rows, sidx]), st)
+            assert (res["status"] == 0).all() and (res["method"] == 2).all()
+            out[cells] = g
+        assert ctx._L.lcbi_gpu_set_grad_resolution(ctx.handle, 4) != 0
+    finally:
+        ctx._L.lcbi_gpu_set_grad_resolution(ctx.handle, 48)
+    ref = out[192]
+    assert np.isfinite(ref[:, :7]).all()
+    rho = rows[:, 4]
+    # dA/d(y1, y2, rho) scaled by rho, dA/ds by s, relative to the magnification
+    scale = np.column_stack([rho, rho, rows[:, 0], rho]) / ref[:, 6:7]
+    cols = [0, 1, 2, 4]
+
+    def dev(cells):
+        d = np.abs(out[cells][:, cols] - ref[:, cols]) * scale
+        return np.median(d), np.median(np.abs(out[cells][:, 6] / ref[:, 6] - 1.0))
+
+    g48, a48 = dev(48)
+    g96, a96 = dev(96)
+    assert g96 < 0.6 * g48 and a96 < 0.6 * a48, (g48, g96, a48, a96)

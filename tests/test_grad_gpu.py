@@ -10,7 +10,8 @@ scaled by the parameter's size; 1e-2 at the 75th percentile, the rest from
 kinks of the piecewise-linear approximation and lattice squares joining the
 visited set); that value agrees with the lattice forward to 2e-2,
 and the source-position and rho gradients match finite differences of the
-converged lattice forward (nbin 200, steps of 0.05 rho) to 3e-2 (median).
+converged lattice forward (nbin 200, steps of 0.05 rho) to 1e-2 (median;
+about 2e-3 measured, which the lattice forward's own differences set).
 The rho gradient is not compared with differences of the continuum value:
 its lattice spacing is rho / 50, so a relative change of rho of 1e-4 moves
 lattice vertices a unit away from the origin by about one spacing, and those
@@ -174,7 +175,7 @@ def test_inverse_ray_gradient_matches_converged_forward():
         ru, rd, _, _ = _fd(rows, sidx, st, k, h)
         fd = (ru["magnification"] - rd["magnification"]) / (2 * h)
         err = np.abs(g[:, k] - fd) * size / A
-        assert np.median(err) < 3e-2, (k, np.median(err), np.max(err))
+        assert np.median(err) < 1e-2, (k, np.median(err), np.max(err))
 
 
 def test_light_curve_autograd_matches_finite_differences():
